@@ -1,0 +1,366 @@
+/*
+ * Driver around the reference's own step routines (compiled from
+ * pllcart3d.c / pll_tridiag.c into oracle/_ref/ by oracle/Makefile).
+ * Test infrastructure only: it exists so that the CPU restatement in
+ * oracle/pllcart3d_oracle.c can be pinned against the reference itself and so
+ * that the reference CPU path can be timed.  It is never part of the GPU
+ * library.
+ *
+ * pllref_init mirrors main() start-up (pllcart3d.c:57-73); pllref_load_ic
+ * replaces initial_condition (pllcart3d.c:80) by caller-supplied arrays and
+ * then runs pllcart3d.c:81-83 and 126-154; pllref_steps runs the time-step
+ * body pllcart3d.c:158-195 a fixed number of times (diagnostics and file
+ * output of pllcart3d.c:198-256 are left out).
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+#include "structures_3d.h"
+
+/* reference globals (global_variables.h, pllcart3d.c:36) */
+extern int Nx_cell_global, Ny_cell_global, Nz_cell_global;
+extern int Nx_ghost, Ny_ghost, Nz_ghost;
+extern int Initial, Ugrid, Niter_print, Wavpert, Subharm, Nmvp;
+extern double X1, X2, Y1, Y2, Z1, Z2;
+extern double Re, Pe, Vratio, Fx, Fy, Inf_pos, Inf_thick;
+extern double CFLmax, Timemax, Timestep, Out_inter, Out_mid;
+extern double PI, M, Vnorm, Ampli, Lamb, Mum, Lambda;
+extern double RK1[3], RK2[3];
+extern int Rank, Size;
+
+/* reference routines (global_function_decl.h, allocate_3d_calloc.h) */
+void input();
+void grid_setup(Grid *);
+void simulation_setup(Grid *, Velo *, Velo *, Velo *, Conc *);
+void mesh_generation(Grid *);
+void plan_dct_3d(int, int, int);
+void fdct_3d(int, int, int, double ***, double ***);
+void idct_3d(int, int, int, double ***, double ***);
+Velo *alloc_velo(int, int, int);
+Conc *alloc_conc(int, int, int);
+Visc *alloc_visc(int, int, int);
+double ***alloc3d_dble(int, int, int);
+Tds *alloc_tds(int, int);
+void free_tds(Tds *, int, int);
+void pll_tridiag(Tds *, int, int);
+int tridiag_1rhs(int, double *, double *, double *, double *);
+double calculate_weno(double *, int, int);
+void concentration(double, double, double, double, Grid *, double ***,
+                   double ***, double ***, Conc *);
+double slope_parameter(Grid *, double ***);
+void calculate_viscosity(Grid *, double ***, Visc *);
+void calculate_viscosity_nmvp(Grid *, double ***, Visc *, double);
+void xmom(double, double, double, double, Grid *, Visc *, Visc *, double ***,
+          double ***, double ***, Velo *);
+void ymom(double, double, double, double, Grid *, Visc *, Visc *, double ***,
+          double ***, double ***, Velo *);
+void zmom(double, double, double, double, Grid *, Visc *, Visc *, double ***,
+          double ***, Velo *);
+void A_conc(Grid *, Conc *);
+void A_umom(Grid *, Visc *, Velo *);
+void A_vmom(Grid *, Visc *, Velo *);
+void A_wmom(Grid *, Visc *, Velo *);
+void divergence(Grid *, double ***, double ***, double ***, double ***);
+void phisolver_dct(double, double, double, Grid *, double ***, double ***);
+void velo_correction(double, double, double, Grid *, double ***, Velo *,
+                     Velo *, Velo *);
+void update_veloghost_points(Grid *, Velo *, Velo *, Velo *);
+void update_ghost_points(Grid *, double ***, Velo *, Velo *, Velo *);
+void update_velo_boundary(Grid *, Velo *, Velo *, Velo *);
+void update_phi_ghosts(Grid *, double ***);
+void pressure_gradient(double, double, double, Grid *, double ***, Velo *,
+                       Velo *, Velo *);
+double find_cfl(Grid *, double ***, double ***, double ***);
+double bulk_velo(Grid *, double ***);
+void update_old_conc(Conc *);
+void update_old_velo(Velo *, Velo *, Velo *);
+void update_old_visc(Visc *, Visc *);
+void pll_shim_fftw_set_fast(int);
+
+static Grid *g_grid;
+static Velo *g_u, *g_v, *g_w;
+static Conc *g_c;
+static Visc *g_mu_old, *g_mu_new;
+static double ***g_phi, ***g_div;
+static double g_tval, g_dt, g_cm;
+
+int pllref_init(const char *rundir)
+{
+    char here[4096];
+    if (!getcwd(here, sizeof(here))) return -1;
+    if (chdir(rundir) != 0) return -1;
+    Rank = 0;
+    Size = 1;
+    input();
+    g_grid = (Grid *)malloc(sizeof(Grid));
+    grid_setup(g_grid);
+    g_u = alloc_velo(g_grid->nx_max, g_grid->ny_max, g_grid->nz_max);
+    g_v = alloc_velo(g_grid->nx_max, g_grid->ny_max, g_grid->nz_max);
+    g_w = alloc_velo(g_grid->nx_max, g_grid->ny_max, g_grid->nz_max);
+    g_c = alloc_conc(g_grid->nx_max, g_grid->ny_max, g_grid->nz_max);
+    g_mu_old = alloc_visc(g_grid->nx_max, g_grid->ny_max, g_grid->nz_max);
+    g_mu_new = alloc_visc(g_grid->nx_max, g_grid->ny_max, g_grid->nz_max);
+    g_phi = alloc3d_dble(g_grid->nx_max, g_grid->ny_max, g_grid->nz_max);
+    g_div = alloc3d_dble(g_grid->nx_max, g_grid->ny_max, g_grid->nz_max);
+    simulation_setup(g_grid, g_u, g_v, g_w, g_c);
+    mesh_generation(g_grid);
+    plan_dct_3d(g_grid->ny_cell, g_grid->nz_cell, g_grid->nx_cell);
+    g_tval = 0.0;
+    if (chdir(here) != 0) return -1;
+    return 0;
+}
+
+void pllref_set_fast_dct(int fast) { pll_shim_fftw_set_fast(fast); }
+
+void pllref_dims(int *d)
+{
+    d[0] = g_grid->nx_max;
+    d[1] = g_grid->ny_max;
+    d[2] = g_grid->nz_max;
+    d[3] = g_grid->nx_cell;
+    d[4] = g_grid->ny_cell;
+    d[5] = g_grid->nz_cell;
+}
+
+static double ***field(const char *name)
+{
+    if (!strcmp(name, "c_old")) return g_c->old;
+    if (!strcmp(name, "c_new")) return g_c->new;
+    if (!strcmp(name, "c_hn")) return g_c->explicit_n;
+    if (!strcmp(name, "c_hnm1")) return g_c->explicit_nm1;
+#define VEL(P, V)                                                   \
+    if (!strcmp(name, P "_old")) return V->old;                     \
+    if (!strcmp(name, P "_new")) return V->new;                     \
+    if (!strcmp(name, P "_hn")) return V->explicit_n;               \
+    if (!strcmp(name, P "_hnm1")) return V->explicit_nm1;           \
+    if (!strcmp(name, P "_pg")) return V->pg;
+    VEL("u", g_u)
+    VEL("v", g_v)
+    VEL("w", g_w)
+#undef VEL
+#define MU(P, V)                                                    \
+    if (!strcmp(name, P "_cell")) return V->cell;                   \
+    if (!strcmp(name, P "_xy")) return V->xy;                       \
+    if (!strcmp(name, P "_xz")) return V->xz;                       \
+    if (!strcmp(name, P "_yz")) return V->yz;
+    MU("mu_old", g_mu_old)
+    MU("mu_new", g_mu_new)
+#undef MU
+    if (!strcmp(name, "phi")) return g_phi;
+    if (!strcmp(name, "div")) return g_div;
+    return NULL;
+}
+
+static Tri_abc ***abc_field(const char *name)
+{
+    if (!strcmp(name, "c_Ax")) return g_c->Ax;
+    if (!strcmp(name, "c_Ay")) return g_c->Ay;
+    if (!strcmp(name, "c_Az")) return g_c->Az;
+    if (!strcmp(name, "u_Ax")) return g_u->Ax;
+    if (!strcmp(name, "u_Ay")) return g_u->Ay;
+    if (!strcmp(name, "u_Az")) return g_u->Az;
+    if (!strcmp(name, "v_Ax")) return g_v->Ax;
+    if (!strcmp(name, "v_Ay")) return g_v->Ay;
+    if (!strcmp(name, "v_Az")) return g_v->Az;
+    if (!strcmp(name, "w_Ax")) return g_w->Ax;
+    if (!strcmp(name, "w_Ay")) return g_w->Ay;
+    if (!strcmp(name, "w_Az")) return g_w->Az;
+    return NULL;
+}
+
+int pllref_get(const char *name, double *out)
+{
+    int i, j, NY = g_grid->ny_max, NZ = g_grid->nz_max;
+    double ***f = field(name);
+    if (!f) return -1;
+    for (i = 0; i < g_grid->nx_max; i++)
+        for (j = 0; j < NY; j++)
+            memcpy(out + ((long)i * NY + j) * NZ, f[i][j], sizeof(double) * NZ);
+    return 0;
+}
+
+int pllref_set(const char *name, const double *in)
+{
+    int i, j, NY = g_grid->ny_max, NZ = g_grid->nz_max;
+    double ***f = field(name);
+    if (!f) return -1;
+    for (i = 0; i < g_grid->nx_max; i++)
+        for (j = 0; j < NY; j++)
+            memcpy(f[i][j], in + ((long)i * NY + j) * NZ, sizeof(double) * NZ);
+    return 0;
+}
+
+/* coefficient triples on the variable's own interior range only (the rest of
+ * a Tri_abc row is uninitialised malloc memory, allocate_3d_calloc.h:97) */
+int pllref_get_abc(const char *name, int is, int ie, int js, int je, int ks,
+                   int ke, double *a, double *b, double *c)
+{
+    int i, j, k, NY = g_grid->ny_max, NZ = g_grid->nz_max;
+    Tri_abc ***f = abc_field(name);
+    if (!f) return -1;
+    for (i = is; i <= ie; i++)
+        for (j = js; j <= je; j++)
+            for (k = ks; k <= ke; k++) {
+                long id = ((long)i * NY + j) * NZ + k;
+                a[id] = f[i][j][k].a;
+                b[id] = f[i][j][k].b;
+                c[id] = f[i][j][k].c;
+            }
+    return 0;
+}
+
+/* pllcart3d.c:81-83 and 126-154 after caller-supplied initial fields */
+int pllref_load_ic(const double *c, const double *u, const double *v,
+                   const double *w)
+{
+    double del_min, diff_dt;
+    pllref_set("c_new", c);
+    pllref_set("u_new", u);
+    pllref_set("v_new", v);
+    pllref_set("w_new", w);
+    update_ghost_points(g_grid, g_phi, g_u, g_v, g_w);
+    update_old_conc(g_c);
+    update_old_velo(g_u, g_v, g_w);
+    if (Nmvp == 1) {
+        g_cm = slope_parameter(g_grid, g_c->new);
+        calculate_viscosity_nmvp(g_grid, g_c->old, g_mu_old, g_cm);
+    } else {
+        calculate_viscosity(g_grid, g_c->old, g_mu_old);
+    }
+    A_conc(g_grid, g_c);
+    A_umom(g_grid, g_mu_old, g_u);
+    A_vmom(g_grid, g_mu_old, g_v);
+    A_wmom(g_grid, g_mu_old, g_w);
+    del_min = (g_grid->dx < g_grid->dy) ? g_grid->dx : g_grid->dy;
+    del_min = (del_min < g_grid->dz) ? del_min : g_grid->dz;
+    diff_dt = 0.1 * Pe * del_min * del_min;
+    Timestep = (diff_dt < Timestep) ? diff_dt : Timestep;
+    g_tval = 0.0;
+    return 0;
+}
+
+/* one RK3-CN substep, pllcart3d.c:164-194 */
+void pllref_substep(double dt, int rkstep)
+{
+    double g = RK1[rkstep], r = RK2[rkstep], vbulk = 0.0;
+    g_tval = g_tval + (g + r) * dt;
+    vbulk = bulk_velo(g_grid, g_u->old);
+    concentration(dt, g, r, vbulk, g_grid, g_u->new, g_v->new, g_w->new, g_c);
+    if (Nmvp == 1)
+        calculate_viscosity_nmvp(g_grid, g_c->new, g_mu_new, g_cm);
+    else
+        calculate_viscosity(g_grid, g_c->new, g_mu_new);
+    xmom(dt, g, r, vbulk, g_grid, g_mu_old, g_mu_new, g_c->new, g_v->old,
+         g_w->old, g_u);
+    ymom(dt, g, r, vbulk, g_grid, g_mu_old, g_mu_new, g_c->new, g_u->old,
+         g_w->old, g_v);
+    zmom(dt, g, r, vbulk, g_grid, g_mu_old, g_mu_new, g_u->old, g_v->old, g_w);
+    update_velo_boundary(g_grid, g_u, g_v, g_w);
+    divergence(g_grid, g_u->new, g_v->new, g_w->new, g_div);
+    phisolver_dct(dt, g, r, g_grid, g_div, g_phi);
+    update_phi_ghosts(g_grid, g_phi);
+    velo_correction(dt, g, r, g_grid, g_phi, g_u, g_v, g_w);
+    update_veloghost_points(g_grid, g_u, g_v, g_w);
+    pressure_gradient(dt, g, r, g_grid, g_phi, g_u, g_v, g_w);
+    update_old_conc(g_c);
+    update_old_velo(g_u, g_v, g_w);
+    update_old_visc(g_mu_old, g_mu_new);
+}
+
+double pllref_step_dt(void)
+{
+    double cfl_dt = find_cfl(g_grid, g_u->old, g_v->old, g_w->old);
+    return (cfl_dt < Timestep) ? cfl_dt : Timestep;
+}
+
+/* pllcart3d.c:158-195, n times */
+int pllref_steps(int n)
+{
+    int s, rk;
+    for (s = 0; s < n; s++) {
+        g_dt = pllref_step_dt();
+        for (rk = 0; rk < 3; rk++) pllref_substep(g_dt, rk);
+    }
+    return 0;
+}
+
+double pllref_last_dt(void) { return g_dt; }
+double pllref_tval(void) { return g_tval; }
+double pllref_timestep(void) { return Timestep; }
+
+/* single routines, for per-routine parity */
+void pllref_concentration(double dt, double g, double r, double vb)
+{
+    concentration(dt, g, r, vb, g_grid, g_u->new, g_v->new, g_w->new, g_c);
+}
+void pllref_viscosity_new(void) { calculate_viscosity(g_grid, g_c->new, g_mu_new); }
+void pllref_xmom(double dt, double g, double r, double vb)
+{
+    xmom(dt, g, r, vb, g_grid, g_mu_old, g_mu_new, g_c->new, g_v->old, g_w->old, g_u);
+}
+void pllref_ymom(double dt, double g, double r, double vb)
+{
+    ymom(dt, g, r, vb, g_grid, g_mu_old, g_mu_new, g_c->new, g_u->old, g_w->old, g_v);
+}
+void pllref_zmom(double dt, double g, double r, double vb)
+{
+    zmom(dt, g, r, vb, g_grid, g_mu_old, g_mu_new, g_u->old, g_v->old, g_w);
+}
+void pllref_update_velo_boundary(void) { update_velo_boundary(g_grid, g_u, g_v, g_w); }
+void pllref_divergence(void) { divergence(g_grid, g_u->new, g_v->new, g_w->new, g_div); }
+void pllref_phisolver(double dt, double g, double r) { phisolver_dct(dt, g, r, g_grid, g_div, g_phi); }
+void pllref_update_phi_ghosts(void) { update_phi_ghosts(g_grid, g_phi); }
+void pllref_velo_correction(double dt, double g, double r)
+{
+    velo_correction(dt, g, r, g_grid, g_phi, g_u, g_v, g_w);
+}
+void pllref_update_veloghost_points(void) { update_veloghost_points(g_grid, g_u, g_v, g_w); }
+void pllref_pressure_gradient(double dt, double g, double r)
+{
+    pressure_gradient(dt, g, r, g_grid, g_phi, g_u, g_v, g_w);
+}
+void pllref_rotate(void)
+{
+    update_old_conc(g_c);
+    update_old_velo(g_u, g_v, g_w);
+    update_old_visc(g_mu_old, g_mu_new);
+}
+void pllref_rebuild_A_old(void)
+{
+    A_umom(g_grid, g_mu_old, g_u);
+    A_vmom(g_grid, g_mu_old, g_v);
+    A_wmom(g_grid, g_mu_old, g_w);
+}
+double pllref_find_cfl(void) { return find_cfl(g_grid, g_u->old, g_v->old, g_w->old); }
+double pllref_bulk_velo(void) { return bulk_velo(g_grid, g_u->old); }
+
+/* batched line solves through the reference's pll_tridiag / tridiag_1rhs */
+void pllref_pll_tridiag(int N, int n, double *a, double *b, double *c, double *r)
+{
+    int s;
+    Tds *t = alloc_tds(N, n);
+    for (s = 0; s < N; s++) {
+        memcpy(t[s].acof, a + (long)s * n, sizeof(double) * n);
+        memcpy(t[s].bcof, b + (long)s * n, sizeof(double) * n);
+        memcpy(t[s].ccof, c + (long)s * n, sizeof(double) * n);
+        memcpy(t[s].rhs, r + (long)s * n, sizeof(double) * n);
+    }
+    pll_tridiag(t, N, n);
+    for (s = 0; s < N; s++) {
+        memcpy(b + (long)s * n, t[s].bcof, sizeof(double) * n);
+        memcpy(c + (long)s * n, t[s].ccof, sizeof(double) * n);
+        memcpy(r + (long)s * n, t[s].rhs, sizeof(double) * n);
+    }
+    free_tds(t, N, n);
+}
+int pllref_tridiag_1rhs(int n, double *a, double *b, double *c, double *r)
+{
+    return tridiag_1rhs(n, a, b, c, r);
+}
+double pllref_calculate_weno(double *d1, int kk, int sign)
+{
+    return calculate_weno(d1, kk, sign);
+}
