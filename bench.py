@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Throughput of the pllcart3d time step on B200, in cell-steps/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME]
+
+One step = one full RK3-CN time step (pllcart3d.c:158-195) of the named
+seeded synthetic fingering workload (default fingering-512x256x256, the size
+the headline metric is quoted at).  The FP64 state arrays are each 282 MB,
+larger than the 126 MB L2, so no L2 flush is needed between steps.
+
+--impl ours       the GPU step through the pllgpu_ C ABI (one CUDA graph per
+                  step); `value` is device-timed with CUDA events on the
+                  solver's stream, max over ranks; `e2e` goes through
+                  pllgpu_run_host with pinned host buffers (initial fields
+                  in, c/u/v/w out, inside the timed region).
+--impl reference  the reference's own CPU step (pllcart3d.c compiled by
+                  oracle/Makefile, single rank), timed on the host cores on a
+                  bounded sample of steps of the same workload.
+With N>1 (torchrun) every rank advances its own replica (the north-star path
+runs on one GPU; replicas only) and `value` sums cells over ranks.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from pllcart3d_b200 import roofline  # noqa: E402
+from pllcart3d_b200.ic import workload_fields  # noqa: E402
+from pllcart3d_b200.params import workload  # noqa: E402
+
+METRIC = "cell-steps/s"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="fingering-512x256x256")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def reduce_max(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def peaks():
+    try:
+        with open(PEAKS) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            out = ""
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample(wl_name, seconds=12.0):
+    """The reference CPU step (oracle/_ref, else the CPU restatement) on a
+    bounded sample: a 64x32x32 grid of the workload's physics, stepped until
+    ~`seconds` of single-core work; returns (cell-steps/s, kind, sample)."""
+    from oracle.pyref import OracleRun, RefRun, ref_available
+
+    wl = workload(wl_name)
+    small = wl.params.replace(Nx_cell_global=64, Ny_cell_global=32, Nz_cell_global=32)
+    ic = workload_fields(type(wl)(wl.name, small, wl.modes, wl.amplitude, wl.steps, wl.seed))
+    if ref_available():
+        run, kind = RefRun(small, ic), "reference"
+        run.set_fast_dct(True)
+    else:
+        run, kind = OracleRun(small, ic), "port"
+        run.set_fast_dct(True)
+    run.steps(1)
+    t0 = time.perf_counter()
+    n = 0
+    while time.perf_counter() - t0 < seconds:
+        run.steps(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    cells = small.cells
+    sample = (f"{n} steps of a 64x32x32 grid with the {wl.name} physics, "
+              f"single core, FFT-based DCT stand-in for FFTW")
+    return cells * n / dt, kind, sample, n
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    wl = workload(args.workload)
+    vals = []
+    # warm-up and timed steps, each a bounded sample of the workload
+    for s in range(args.warmup + args.steps):
+        v, kind, sample, n = cpu_sample(args.workload, seconds=2.0)
+        if s >= args.warmup:
+            vals.append(v)
+    value = statistics.mean(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl.name, "grid": [wl.params.nx, wl.params.ny, wl.params.nz],
+                   "precision": "fp64"},
+        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": 1,
+                         "kind": kind, "sample": sample + " per step"},
+        "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, ws, rank, local):
+    import numpy as np
+    import torch
+
+    from pllcart3d_b200 import _lib
+    from pllcart3d_b200.solver import Solver
+
+    torch.cuda.set_device(local)
+    wl = workload(args.workload)
+    prm = wl.params
+    cells = prm.cells
+    ic = workload_fields(wl)
+    s = Solver(prm, device=local, exact_dct=True, use_graph=True)
+    s.load_ic(ic)
+    stream = torch.cuda.ExternalStream(s._L.pllgpu_stream(s._h), device=local)
+
+    s.step(args.warmup)
+    barrier(ws)
+    clocks = Clocks(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    ms = e0.elapsed_time(e1)
+    ck = clocks.stop()
+    ms_max = reduce_max(ms, ws)
+    value = cells * args.steps * ws / (ms_max / 1e3)
+    launches = s.kernels_per_step * args.steps
+
+    # per-kernel device times of the same step (stream launches + events)
+    import ctypes
+
+    maxk = 64
+    names = ctypes.create_string_buffer(32 * maxk)
+    tot = (ctypes.c_double * maxk)()
+    cnt = (ctypes.c_int * maxk)()
+    nk = ctypes.c_int(0)
+    nprof = 2
+    code = s._L.pllgpu_profile_steps(s._h, nprof, maxk, names, tot, cnt, ctypes.byref(nk))
+    kernels = {}
+    if code == 0:
+        for t in range(nk.value):
+            lab = names.raw[32 * t:32 * t + 32].split(b"\0")[0].decode()
+            kernels[lab] = {"ms_total": tot[t], "launches": cnt[t]}
+    step_ms_prof = sum(v["ms_total"] for v in kernels.values()) / nprof
+    hbm, peak_kind = peaks()
+    roof = None
+    cand = {k: v for k, v in kernels.items() if k in roofline.KERNEL_WORDS}
+    if cand:
+        top = max(cand, key=lambda k: cand[k]["ms_total"])
+        avg_ms = cand[top]["ms_total"] / cand[top]["launches"]
+        alg = roofline.kernel_bytes_per_launch(top, cells)
+        ach = alg / (avg_ms / 1e3) / 1e9
+        roof = {"kernel": top, "bound": "hbm", "achieved": ach, "peak": hbm,
+                "unit": "GB/s", "frac": ach / hbm, "traffic": None,
+                "peak_source": peak_kind,
+                "share_of_step": cand[top]["ms_total"] / nprof / step_ms_prof}
+    step_bytes = roofline.step_bytes(cells)
+    step_roof = {"bytes_per_step": step_bytes,
+                 "achieved_gbs": step_bytes / (ms / args.steps / 1e3) / 1e9,
+                 "frac_of_hbm": step_bytes / (ms / args.steps / 1e3) / 1e9 / hbm}
+
+    e2e = None
+    if not args.no_e2e:
+        shape = prm.shape
+        pin = [torch.empty(shape, dtype=torch.float64, pin_memory=True) for _ in range(8)]
+        for t, k in zip(pin[:4], "cuvw"):
+            t.numpy()[...] = ic[k]
+        ptr = [ctypes.cast(t.data_ptr(), ctypes.POINTER(ctypes.c_double)) for t in pin]
+        s2 = s
+        t0 = time.perf_counter()
+        code = s2._L.pllgpu_run_host(s2._h, args.steps, *ptr)
+        t1 = time.perf_counter()
+        if code != 0:
+            raise _lib.PllGpuError(code, "run_host")
+        sec = reduce_max(t1 - t0, ws)
+        nbytes = 4 * int(np.prod(shape)) * 8
+        e2e = {"value": cells * args.steps * ws / sec, "unit": "cell-steps/s",
+               "h2d_bytes_per_step": nbytes / args.steps,
+               "d2h_bytes_per_step": nbytes / args.steps,
+               "note": "pllgpu_run_host: initial c,u,v,w from pinned host memory, "
+                       f"{args.steps} steps, c,u,v,w back to pinned host memory, "
+                       "wall-clock around the call"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            v, kind, sample, n = cpu_sample(args.workload, seconds=12.0)
+            cpu = {"value": v, "unit": "cell-steps/s", "cores": 1, "kind": kind,
+                   "sample": sample}
+        except Exception as ex:  # the checker may be absent on a bare box
+            cpu = {"value": None, "unit": "cell-steps/s", "cores": 1, "kind": "none",
+                   "sample": f"unavailable: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl.name, "grid": [prm.nx, prm.ny, prm.nz],
+                       "precision": "fp64", "parallelism": "replicas" if ws > 1 else "single",
+                       "l2": "inputs larger than L2 (282 MB per field)"},
+            "e2e": e2e, "gpu_launches": launches, "roofline": roof,
+            "step_roofline": step_roof, "cpu_baseline": cpu, "clocks": ck,
+            "kernels_ms_per_step": {k: v["ms_total"] / nprof for k, v in kernels.items()},
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

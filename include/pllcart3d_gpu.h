@@ -1,0 +1,236 @@
+/*
+ * pllcart3d_gpu.h - C ABI of the B200 implementation of pllcart3d's
+ * RK3 / Crank-Nicolson time step (csdms-contrib/pllcart3d).
+ *
+ * Two layers, both plain C:
+ *
+ * 1. The device API (libpllgpu.so, prefix pllgpu_): a context that owns the
+ *    solver state in HBM, runs whole time steps on the GPU (one CUDA graph
+ *    per step) and runs each step routine of the reference on its own for
+ *    per-routine parity.  Fields cross the boundary as contiguous float64
+ *    arrays over the padded box (nx+6) x (ny+2) x (nz+2), z fastest - the
+ *    element order of the reference's double***[i][j][k] arrays
+ *    (allocate_3d_calloc.h:46-64).
+ *
+ * 2. The drop-in layer (libpllcart3d_dropin.so): the reference's own
+ *    step-routine names and signatures (global_function_decl.h:7-26,36-42,
+ *    pll_tridiag.c:152, fftw_3d.h:3-5) over its structures_3d.h types, so
+ *    that pllcart3d.c links against it in place of its CPU routines.  Those
+ *    prototypes take the reference's Grid/Velo/Conc/Visc/Tds types and are
+ *    declared by the reference's own headers; they are listed at the end of
+ *    this file with layout-identical mirror types (the reference names a
+ *    member `new`, which is why the mirrors rename it).
+ *
+ * Errors: every pllgpu_ call returns PLLGPU_OK or an error code; the status
+ * of a context is sticky until pllgpu_clear_status.  Nothing here traps or
+ * exits the process; the reference's exit(1) paths (NaN in find_max,
+ * pllcart3d.c:3568-3588; slope-parameter non-convergence, L813-818) become
+ * PLLGPU_ENAN / PLLGPU_ENOCONV.
+ */
+#ifndef PLLCART3D_GPU_H
+#define PLLCART3D_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define PLLGPU_OK 0
+#define PLLGPU_ENAN 1      /* NaN/Inf met in the CFL scan (find_max's guard)  */
+#define PLLGPU_ECUDA 2     /* a CUDA call failed                               */
+#define PLLGPU_ETIMEOUT 3  /* a bounded device wait gave up                    */
+#define PLLGPU_EBOUNDS 4   /* a kernel self-check found a bad index            */
+#define PLLGPU_EINVAL 5    /* bad argument (size, field id, routine id)        */
+#define PLLGPU_ENOCONV 6   /* slope_parameter bisection did not converge       */
+
+/* precision forms */
+#define PLLGPU_FP64 0      /* plain: the reference's FP64 arithmetic           */
+
+/* run parameters: the values of param.input that the step reads
+ * (input() pllcart3d.c:271-350); M = Vratio, Vnorm = 0 (L400-403) */
+typedef struct pllgpu_params {
+    int nx, ny, nz;        /* Nx_cell_global, Ny_cell_global, Nz_cell_global */
+    int nmvp;              /* Nmvp: 0 mu = exp(M c), 1 non-monotonic law      */
+    double X1, X2, Y1, Y2, Z1, Z2;
+    double Re, Pe, Vratio, Fx, Fy, CFLmax, Timestep, Mum, Lambda;
+    int precision;         /* PLLGPU_FP64                                      */
+    int exact_dct;         /* 1: DCT sums in sequential order (bitwise with
+                              the CPU restatement); 0: tensor-core DMMA        */
+    int use_graph;         /* 1: replay each step as one CUDA graph            */
+    int reserved[5];
+} pllgpu_params;
+
+typedef struct pllgpu_ctx pllgpu_ctx;
+
+/* field ids (pllgpu_field_id maps the names "c_old" ... "div") */
+enum {
+    PLLGPU_C_OLD = 0, PLLGPU_C_NEW, PLLGPU_C_HN, PLLGPU_C_HNM1,
+    PLLGPU_U_OLD, PLLGPU_U_NEW, PLLGPU_U_HN, PLLGPU_U_HNM1, PLLGPU_U_PG,
+    PLLGPU_V_OLD, PLLGPU_V_NEW, PLLGPU_V_HN, PLLGPU_V_HNM1, PLLGPU_V_PG,
+    PLLGPU_W_OLD, PLLGPU_W_NEW, PLLGPU_W_HN, PLLGPU_W_HNM1, PLLGPU_W_PG,
+    PLLGPU_MU_OLD_CELL, PLLGPU_MU_OLD_XY, PLLGPU_MU_OLD_XZ, PLLGPU_MU_OLD_YZ,
+    PLLGPU_MU_NEW_CELL, PLLGPU_MU_NEW_XY, PLLGPU_MU_NEW_XZ, PLLGPU_MU_NEW_YZ,
+    PLLGPU_PHI, PLLGPU_DIV,
+    PLLGPU_NFIELDS
+};
+
+/* routine ids for pllgpu_routine; scalars in[] as listed, out[0] result */
+enum {
+    PLLGPU_R_CONCENTRATION = 0,   /* concentration L555-719: dt,g,r,vbulk     */
+    PLLGPU_R_VISCOSITY_NEW,       /* calculate_viscosity(c_new) L843-886      */
+    PLLGPU_R_XMOM,                /* xmom L952-1107: dt,g,r,vbulk             */
+    PLLGPU_R_YMOM,                /* ymom L1110-1260                          */
+    PLLGPU_R_ZMOM,                /* zmom L1263-1408                          */
+    PLLGPU_R_VELO_GHOSTS,         /* update_velo_boundary L2701-2755 /
+                                     update_veloghost_points L2810-2885       */
+    PLLGPU_R_DIVERGENCE,          /* divergence L1983-1999                    */
+    PLLGPU_R_PHISOLVER,           /* phisolver_dct L2002-2130: dt,g,r         */
+    PLLGPU_R_PHI_GHOSTS,          /* update_phi_ghosts L2758-2807             */
+    PLLGPU_R_VELO_CORRECTION,     /* velo_correction L2133-2227: dt,g,r       */
+    PLLGPU_R_PRESSURE_GRADIENT,   /* pressure_gradient L2964-3044: dt,g,r     */
+    PLLGPU_R_ROTATE,              /* update_old_conc/velo/visc L3402-3452     */
+    PLLGPU_R_BULK_VELO,           /* bulk_velo L3381-3398 -> out[0]           */
+    PLLGPU_R_FIND_CFL,            /* find_cfl L3095-3118 -> out[0]            */
+    PLLGPU_R_SUBSTEP,             /* one RK substep L164-194: dt, rk          */
+    PLLGPU_NROUTINES
+};
+
+pllgpu_ctx *pllgpu_create(const pllgpu_params *p, int device);
+void pllgpu_destroy(pllgpu_ctx *ctx);
+int pllgpu_field_id(const char *name);
+int pllgpu_dims(const pllgpu_ctx *ctx, int *dims6); /* NX NY NZ nx ny nz */
+int pllgpu_set_field(pllgpu_ctx *ctx, int field, const double *host);
+int pllgpu_get_field(pllgpu_ctx *ctx, int field, double *host);
+/* device address and element strides (i, j) of a field in the current
+ * roles; valid until the next step or rotate */
+int pllgpu_device_field(pllgpu_ctx *ctx, int field, double **dptr,
+                        long *stride_i, long *stride_j);
+/* start-up after the initial *_new fields are set: pllcart3d.c:81-83
+ * (ghost fill, new -> old), 126-148 (viscosity of c_old, slope parameter)
+ * and 150-154 (diffusive cap of Timestep) */
+int pllgpu_start(pllgpu_ctx *ctx);
+/* n full time steps, pllcart3d.c:158-195, dt from the device CFL scan */
+int pllgpu_steps(pllgpu_ctx *ctx, int nsteps);
+/* n steps, copying the four initial fields in from host and c,u,v,w out to
+ * host inside the call (end-to-end entry point) */
+int pllgpu_run_host(pllgpu_ctx *ctx, int nsteps, const double *c0,
+                    const double *u0, const double *v0, const double *w0,
+                    double *c, double *u, double *v, double *w);
+int pllgpu_routine(pllgpu_ctx *ctx, int routine, const double *in, double *out);
+int pllgpu_sync(pllgpu_ctx *ctx);
+int pllgpu_status(const pllgpu_ctx *ctx);
+void pllgpu_clear_status(pllgpu_ctx *ctx);
+double pllgpu_last_dt(pllgpu_ctx *ctx);
+double pllgpu_timestep(const pllgpu_ctx *ctx);
+double pllgpu_tval(pllgpu_ctx *ctx);
+const char *pllgpu_error_string(int code);
+/* number of kernel launches one time step issues */
+int pllgpu_kernels_per_step(const pllgpu_ctx *ctx);
+/* the CUDA stream (cudaStream_t) every kernel of the context runs on */
+void *pllgpu_stream(pllgpu_ctx *ctx);
+/* nsteps steps launched one kernel at a time with a CUDA event after each
+ * launch: per kernel label (names: maxk slots of 32 chars) the summed
+ * device time in ms and the number of launches; *nk = labels filled */
+int pllgpu_profile_steps(pllgpu_ctx *ctx, int nsteps, int maxk, char *names,
+                         double *total_ms, int *launches, int *nk);
+
+/*
+ * Batched line solve of pll_tridiag (pll_tridiag.c:152-158) on one rank:
+ * N independent systems of length n, a/b/c/r each N*n contiguous host
+ * doubles (system s at offset s*n); on return r holds the solution and b, c
+ * the eliminated coefficients, as the reference leaves them.
+ */
+int pllgpu_tridiag_batch(int N, int n, const double *a, double *b, double *c,
+                         double *r);
+
+/*
+ * Batched 2-d DCT of fftw_3d.h:45-106: `howmany` row-major n0 x n1 arrays
+ * (n1 fastest), kind 0 = REDFT10 (DCT-II), 1 = REDFT01 (DCT-III), both
+ * unnormalised as FFTW defines them.  Host buffers.
+ */
+int pllgpu_dct2d_batch(int kind, int n0, int n1, int howmany, const double *in,
+                       double *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Drop-in layer (libpllcart3d_dropin.so).                                   */
+/* The reference's own prototypes, over its structures_3d.h types, are:      */
+/*   void concentration(double,double,double,double,Grid*,double***,        */
+/*                      double***,double***,Conc*);          pllcart3d.c:555 */
+/*   void calculate_viscosity(Grid*,double***,Visc*);         pllcart3d.c:843 */
+/*   void calculate_viscosity_nmvp(Grid*,double***,Visc*,double);       L889 */
+/*   double slope_parameter(Grid*,double***);                           L722 */
+/*   void xmom(double,double,double,double,Grid*,Visc*,Visc*,double***,     */
+/*             double***,double***,Velo*);                               L952 */
+/*   void ymom(...same as xmom...);                                    L1110 */
+/*   void zmom(double,double,double,double,Grid*,Visc*,Visc*,double***,     */
+/*             double***,Velo*);                                        L1263 */
+/*   void A_conc(Grid*,Conc*);  void A_umom(Grid*,Visc*,Velo*);       L1411 */
+/*   void A_vmom(Grid*,Visc*,Velo*); void A_wmom(Grid*,Visc*,Velo*);  L1475 */
+/*   void divergence(Grid*,double***,double***,double***,double***);  L1983 */
+/*   void phisolver_dct(double,double,double,Grid*,double***,double***);    */
+/*                                                                  L2002 */
+/*   void velo_correction(double,double,double,Grid*,double***,Velo*,       */
+/*                        Velo*,Velo*);                                L2133 */
+/*   void update_velo_boundary(Grid*,Velo*,Velo*,Velo*);              L2701 */
+/*   void update_phi_ghosts(Grid*,double***);                         L2758 */
+/*   void update_veloghost_points(Grid*,Velo*,Velo*,Velo*);           L2810 */
+/*   void pressure_gradient(double,double,double,Grid*,double***,Velo*,     */
+/*                          Velo*,Velo*);                              L2964 */
+/*   double find_cfl(Grid*,double***,double***,double***);            L3095 */
+/*   double bulk_velo(Grid*,double***);                               L3381 */
+/*   void update_old_conc(Conc*); void update_old_velo(Velo*,Velo*,Velo*);  */
+/*   void update_old_visc(Visc*,Visc*);                          L3402-3452 */
+/*   double calculate_weno(double*,int,int);                          L3455 */
+/*   int tridiag_1rhs(int,double*,double*,double*,double*);           L3511 */
+/*   void pll_tridiag(Tds*,int,int);                     pll_tridiag.c:152 */
+/*   void plan_dct_3d(int,int,int); void fdct_3d(int,int,int,double***,     */
+/*        double***); void idct_3d(int,int,int,double***,double***);        */
+/*                                                            fftw_3d.h:3-5 */
+/* plus the resident-state fast path:                                       */
+/*   int  pllgpu_attach(Grid*,Velo*u,Velo*v,Velo*w,Conc*,Visc*mu_old,       */
+/*                      Visc*mu_new,double***phi);                           */
+/*   int  pllgpu_advance(int nsteps,double *tval);                          */
+/*   int  pllgpu_sync_to_host(void);                                        */
+/*   int  pllgpu_dropin_status(void); void pllgpu_finalize(void);           */
+/* Layout-identical mirrors of the reference types follow.                   */
+/* ------------------------------------------------------------------------ */
+typedef struct pll_tds {          /* Tds, structures_3d.h:2-8 */
+    double *acof, *bcof, *ccof, *rhs;
+} pll_tds;
+typedef struct pll_tri_abc {      /* Tri_abc, structures_3d.h:11-16 */
+    double a, b, c;
+} pll_tri_abc;
+typedef struct pll_velo {         /* Velo, structures_3d.h:19-27 */
+    int nx_max, ny_max, nz_max;
+    int istart, iend, jstart, jend, kstart, kend;
+    double ***next, ***old;       /* `new`, `old` */
+    double ***pg;
+    double ***explicit_n, ***explicit_nm1;
+    pll_tri_abc ***Ax, ***Ay, ***Az;
+} pll_velo;
+typedef struct pll_conc {         /* Conc, structures_3d.h:30-37 */
+    int nx_max, ny_max, nz_max;
+    int istart, iend, jstart, jend, kstart, kend;
+    double ***next, ***old;
+    double ***explicit_n, ***explicit_nm1;
+    pll_tri_abc ***Ax, ***Ay, ***Az;
+} pll_conc;
+typedef struct pll_visc {         /* Visc, structures_3d.h:40-48 */
+    int nx_max, ny_max, nz_max;
+    double ***cell, ***xy, ***xz, ***yz;
+} pll_visc;
+typedef struct pll_grid {         /* Grid, structures_3d.h:50-60 */
+    int istart, iend, jstart, jend, kstart, kend;
+    int nx_cell, ny_cell, nz_cell;
+    int nx_max, ny_max, nz_max;
+    int nmax_xyz, nx_global_offset;
+    double dx, dy, dz;
+    double *X, *Y, *Z;
+    double *Xc, *Yc, *Zc;
+} pll_grid;
+
+#endif

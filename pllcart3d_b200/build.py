@@ -1,0 +1,76 @@
+"""Build recipe for the in-tree native libraries (sm_100a only).
+
+* ``libpllgpu.so``          - CUDA kernels + runtime + the ``pllgpu_`` C ABI;
+  the FP64 step is compiled with ``--fmad=false`` so that no multiply-add is
+  contracted (the reference's own arithmetic has none);
+* ``libpllcart3d_dropin.so`` - the reference-signature drop-in layer (plain C,
+  compiled with gcc because the reference's structures name a member ``new``).
+
+Run ``python -m pllcart3d_b200.build`` or call :func:`build`.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INC = os.path.join(ROOT, "include")
+LIB = os.path.join(HERE, "libpllgpu.so")
+DROPIN = os.path.join(HERE, "libpllcart3d_dropin.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--fmad=false",
+              "-Xcompiler", "-fPIC", "-Xptxas", "-warn-spills"]
+
+CU_SOURCES = ["runtime.cu"]
+HEADERS = ["common.cuh", "step_kernels.cuh", "aux_kernels.cuh", "dct_kernels.cuh"]
+
+
+def _nvcc() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(cand):
+        raise FileNotFoundError("nvcc not found")
+    return cand
+
+
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    deps = [os.path.join(CSRC, f) for f in CU_SOURCES + HEADERS]
+    deps.append(os.path.join(INC, "pllcart3d_gpu.h"))
+    deps.append(__file__)
+    if force or _stale(LIB, deps):
+        objs = []
+        for src in CU_SOURCES:
+            obj = os.path.join(CSRC, src.replace(".cu", ".o"))
+            cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, "-I", INC, "-c",
+                   os.path.join(CSRC, src), "-o", obj]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True)
+            objs.append(obj)
+        cmd = [_nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs]
+        subprocess.run(cmd, check=True)
+        for o in objs:
+            os.remove(o)
+    dsrc = os.path.join(CSRC, "dropin.c")
+    if os.path.exists(dsrc) and (force or _stale(DROPIN, [dsrc, LIB, os.path.join(INC, "pllcart3d_gpu.h")])):
+        cmd = ["gcc", "-O2", "-fPIC", "-shared", "-std=gnu99", "-Wall", "-I", INC,
+               dsrc, "-o", DROPIN, f"-L{HERE}", "-lpllgpu",
+               "-Wl,-rpath,$ORIGIN"]
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

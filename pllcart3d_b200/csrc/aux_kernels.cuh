@@ -1,0 +1,476 @@
+// Viscosity, reductions, projection and ghost-fill kernels of the step.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "step_kernels.cuh"
+
+namespace pll {
+
+// nmvp coefficient slots in the device scalar array
+enum { S_MUM = 8, S_PSI0 = 9, S_PSI1 = 10, S_NMVA = 11 };
+
+template <typename real>
+__device__ __forceinline__ real visc_law(real cavg, const Consts& K, int nmvp,
+                                         const double* __restrict__ scal)
+{
+    if (!nmvp) return (real)exp((double)((real)K.M * (cavg - (real)K.Vnorm)));
+    // calculate_viscosity_nmvp, pllcart3d.c:906-909
+    const double a = scal[S_NMVA], psi0 = scal[S_PSI0], psi1 = scal[S_PSI1];
+    double eta = ((1 + a) * (double)cavg) / (1 + a * (double)cavg);
+    double psi = psi1 * (1 - eta) + psi0 * eta;
+    return (real)(scal[S_MUM] * sin(psi));
+}
+
+// calculate_viscosity (pllcart3d.c:843-886): mu at cell centres on the box
+// padded by one cell, and on the xy / xz / yz edge families.  One thread per
+// (i,j,k) of i in [is-1, ie+1], j in [0, NY-1], k in [0, NZ-1].
+template <typename real>
+__global__ void __launch_bounds__(128) k_viscosity(Geo G, Rng R, Consts K, int nmvp,
+                                                   const real* __restrict__ cn, real* __restrict__ mc,
+                                                   real* __restrict__ mxy, real* __restrict__ mxz,
+                                                   real* __restrict__ myz, const double* __restrict__ scal)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = R.is - 1 + blockIdx.z;
+    if (k >= G.NZ || j >= G.NY) return;
+    const long sx = G.sx, sy = G.sy;
+    const long id = (long)i * sx + (long)j * sy + k;
+    mc[id] = visc_law<real>(cn[id], K, nmvp, scal);
+    const bool in_i = (i >= R.is), in_i2 = (i <= R.ie);
+    const bool jxy = (j >= R.js) & (j <= R.je + 1), jin = (j >= R.js) & (j <= R.je);
+    const bool kin = (k >= R.ks) & (k <= R.ke), kxz = (k >= R.ks) & (k <= R.ke + 1);
+    const real q = (real)0.25;
+    if (in_i & jxy & kin)
+        mxy[id] = visc_law<real>(q * (cn[id - sx - sy] + cn[id - sy] + cn[id - sx] + cn[id]), K, nmvp, scal);
+    if (in_i & jin & kxz)
+        mxz[id] = visc_law<real>(q * (cn[id - sx - 1] + cn[id - 1] + cn[id - sx] + cn[id]), K, nmvp, scal);
+    if (in_i & in_i2 & jxy & kxz)
+        myz[id] = visc_law<real>(q * (cn[id - sy - 1] + cn[id - 1] + cn[id - sy] + cn[id]), K, nmvp, scal);
+}
+
+// find_cfl (pllcart3d.c:3095-3118): max over interior cells of
+// |u|/dx+|v|/dy+|w|/dz at cell centres, reduced exactly through the bit
+// pattern of non-negative doubles; a NaN/Inf raises ST_NAN (the reference's
+// NaN guard lives in find_max, pllcart3d.c:3568-3588)
+template <typename real>
+__global__ void __launch_bounds__(256) k_cfl(Geo G, Rng R, Consts K, const real* __restrict__ u,
+                                             const real* __restrict__ v, const real* __restrict__ w,
+                                             double* scal, int* status)
+{
+    const int k = R.ks + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = R.js + blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = R.is + blockIdx.z;
+    double m = 0.0;
+    if (k <= R.ke && j <= R.je) {
+        const long id = (long)i * G.sx + (long)j * G.sy + k;
+        double uv = 0.5 * ((double)u[id] + (double)u[id + G.sx]);
+        double vv = 0.5 * ((double)v[id] + (double)v[id + G.sy]);
+        double wv = 0.5 * ((double)w[id] + (double)w[id + 1]);
+        double cfl = (fabs(uv) / K.hx) + (fabs(vv) / K.hy) + (fabs(wv) / K.hz);
+        if (!isfinite(cfl)) atomicOr(status, (int)ST_NAN);
+        else m = cfl;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ double sm[8];
+    const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+    const int warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
+    if (lane == 0) sm[warp] = m;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x * blockDim.y) >> 5;
+        m = lane < nw ? sm[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0 && m > 0.0)
+            atomicMax((unsigned long long*)(scal + S_CFLMAX), (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// dt = min(CFLmax / max, Timestep), pllcart3d.c:159-160, 3115; clears the
+// reduction slot for the next step
+__global__ void k_dt(Consts K, double* scal)
+{
+    double maxall = __longlong_as_double((long long)*(unsigned long long*)(scal + S_CFLMAX));
+    double cfldt = K.CFLmax / maxall;
+    double ts = scal[S_TIMESTEP];
+    scal[S_CFLDT] = cfldt;
+    scal[S_DT] = (cfldt < ts) ? cfldt : ts;
+    *(unsigned long long*)(scal + S_CFLMAX) = 0ull;
+}
+
+// bulk_velo (pllcart3d.c:3381-3398): the signed value of the first (j-major,
+// k-minor) entry of largest |u| on the face i = iend; 0 if all are 0.
+// One block.
+template <typename real>
+__global__ void __launch_bounds__(1024) k_bulk_velo(Geo G, Rng R, const real* __restrict__ u, double* scal)
+{
+    const int nyz = (R.je - R.js + 1) * (R.ke - R.ks + 1), nk = R.ke - R.ks + 1;
+    double best = 0.0;
+    int bidx = 0x7fffffff;
+    for (int t = threadIdx.x; t < nyz; t += blockDim.x) {
+        const int j = R.js + t / nk, k = R.ks + t % nk;
+        double a = fabs((double)u[(long)R.ie * G.sx + (long)j * G.sy + k]);
+        if (a > best) { best = a; bidx = t; }
+    }
+    __shared__ double sb[1024];
+    __shared__ int si[1024];
+    sb[threadIdx.x] = best;
+    si[threadIdx.x] = bidx;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            double b2 = sb[threadIdx.x + s];
+            int i2 = si[threadIdx.x + s];
+            if (b2 > sb[threadIdx.x] || (b2 == sb[threadIdx.x] && i2 < si[threadIdx.x])) {
+                sb[threadIdx.x] = b2;
+                si[threadIdx.x] = i2;
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double vb = 0.0;
+        if (sb[0] > 0.0) {
+            const int t = si[0];
+            const int j = R.js + t / nk, k = R.ks + t % nk;
+            vb = (double)u[(long)R.ie * G.sx + (long)j * G.sy + k];
+        }
+        scal[S_VBULK] = vb;
+    }
+}
+
+// inflow/outflow trapezoid fluxes of velo_correction (pllcart3d.c:2171-2223):
+// per y row a sequential sum over z of 0.5*dz*(u_k+u_{k-1}) from k=ks+1,
+// then a sequential sum over y of 0.5*dy*(q_{j-1}+q_j) from j=js+1 (wall
+// half-cells excluded), in the reference's order.  One block.
+template <typename real>
+__global__ void __launch_bounds__(512) k_flux(Geo G, Rng Ru, Consts K, const real* __restrict__ u,
+                                              double* scal)
+{
+    extern __shared__ double qk[];  // 2 * NY
+    const int iin = Ru.is - 1, iout = Ru.ie + 1;
+    const double hdz = 0.5 * K.hz, hdy = 0.5 * K.hy;
+    for (int j = Ru.js + threadIdx.x; j <= Ru.je; j += blockDim.x) {
+        double qi = 0.0, qo = 0.0;
+        const long bi = (long)iin * G.sx + (long)j * G.sy, bo = (long)iout * G.sx + (long)j * G.sy;
+        for (int k = Ru.ks + 1; k <= Ru.ke; ++k) {
+            qi += hdz * ((double)u[bi + k] + (double)u[bi + k - 1]);
+            qo += hdz * ((double)u[bo + k] + (double)u[bo + k - 1]);
+        }
+        qk[j] = qi;
+        qk[G.NY + j] = qo;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double qin = 0.0, qout = 0.0;
+        for (int j = Ru.js + 1; j <= Ru.je; ++j) {
+            qin += hdy * (qk[j - 1] + qk[j]);
+            qout += hdy * (qk[G.NY + j - 1] + qk[G.NY + j]);
+        }
+        scal[S_QIN] = qin;
+        scal[S_QOUT] = qout;
+        scal[S_DEFICIT] = (qin - qout) / K.area;
+    }
+}
+
+// divergence (pllcart3d.c:1983-1999) scaled by Re/(dt alpha)
+// (phisolver_dct L2010-2024) into the compact [x][y][z] Poisson buffer.
+// With `div_out` set, the unscaled divergence also goes to the padded field.
+template <typename real>
+__global__ void __launch_bounds__(128) k_div_rhs(Geo G, Rng R, Consts K, const real* __restrict__ u,
+                                                 const real* __restrict__ v, const real* __restrict__ w,
+                                                 const real* __restrict__ div_in, real* __restrict__ div_out,
+                                                 real* __restrict__ rhs, const double* __restrict__ scal,
+                                                 double alpha, int mode)
+{
+    // mode 0: rhs from u,v,w ; 1: div_out from u,v,w ; 2: rhs from div_in
+    const int k = R.ks + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = R.js + blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = R.is + blockIdx.z;
+    if (k > R.ke || j > R.je) return;
+    const long id = (long)i * G.sx + (long)j * G.sy + k;
+    real d;
+    if (mode == 2) {
+        d = div_in[id];
+    } else {
+        real dvx = over_h<real>(u[id + G.sx] - u[id], K.hx, K.ihx, K.pow2);
+        real dvy = over_h<real>(v[id + G.sy] - v[id], K.hy, K.ihy, K.pow2);
+        real dvz = over_h<real>(w[id + 1] - w[id], K.hz, K.ihz, K.pow2);
+        d = (dvx + dvy + dvz);
+        if (mode == 1) {
+            div_out[id] = d;
+            return;
+        }
+    }
+    const real fac = (real)(K.Re / (scal[S_DT] * alpha));
+    const long c = ((long)(i - R.is) * (R.je - R.js + 1) + (j - R.js)) * (long)(R.ke - R.ks + 1) + (k - R.ks);
+    rhs[c] = fac * d;
+}
+
+// x-direction tridiagonal of each (ky,kz) Poisson mode (phisolver_dct
+// pllcart3d.c:2040-2091): a = c = 1/dx^2, b = -2/dx^2 + lam_y + lam_z,
+// Neumann at the inlet, and at the outlet Neumann except for mode (0,0),
+// whose right ghost holds phi = 0 (the pressure gauge); pll_tridiag's
+// one-rank arithmetic.  One thread per mode; lines of stride ny*nz.
+template <typename real>
+__global__ void __launch_bounds__(128) k_poisson_x(int nx, int ny, int nz, Consts K,
+                                                   const double* __restrict__ lam_y,
+                                                   const double* __restrict__ lam_z,
+                                                   real* __restrict__ hat, real* __restrict__ cc)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ny * nz) return;
+    const int jy = t / nz, kz = t % nz;
+    const long st = (long)ny * nz;
+    const real a = (real)K.dx2i, c = (real)K.dx2i;
+    const real bmid = (real)(-2.0 * K.dx2i + lam_y[jy] + lam_z[kz]);
+    const bool gauge = (jy == 0) && (kz == 0);
+    real cprev = 0, rprev = 0;
+    for (int m = 0; m < nx; ++m) {
+        const long id = t + (long)m * st;
+        real lb = bmid, lr = hat[id];
+        if (m == 0) lb += a;
+        if (m == nx - 1) {
+            if (gauge) lr -= c * (real)0.0;
+            else lb += c;
+        }
+        real cm, rm;
+        if (m == 0) {
+            lb = lb - (real)0.0 * a;
+            cm = c / lb;
+            rm = (lr - (real)0.0 * a) / lb;
+        } else {
+            lb = (lb - cprev * a);
+            cm = c / lb;
+            rm = (lr - rprev * a) / lb;
+        }
+        cc[id] = cm;
+        hat[id] = rm;
+        cprev = cm;
+        rprev = rm;
+    }
+    real xnext = rprev - cprev * (real)0.0;
+    hat[t + (long)(nx - 1) * st] = xnext;
+    for (int m = nx - 2; m >= 0; --m) {
+        const long id = t + (long)m * st;
+        real x = hat[id] - cc[id] * xnext;
+        hat[id] = x;
+        xnext = x;
+    }
+}
+
+// update_phi_ghosts (pllcart3d.c:2758-2807): Neumann copies on the six
+// faces; FACE 0: z faces over (i,j), 1: y faces over (i,k), 2: x faces over
+// (j,k)
+template <int FACE, typename real>
+__global__ void k_phi_ghosts(Geo G, Rng R, real* __restrict__ p)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y;
+    const long sx = G.sx, sy = G.sy;
+    if (FACE == 0) {
+        const int j = R.js + a, i = R.is + b;
+        if (j > R.je) return;
+        const long base = (long)i * sx + (long)j * sy;
+        p[base + R.ks - 1] = p[base + R.ks];
+        p[base + R.ke + 1] = p[base + R.ke];
+    } else if (FACE == 1) {
+        const int k = R.ks + a, i = R.is + b;
+        if (k > R.ke) return;
+        const long base = (long)i * sx + k;
+        p[base + (long)(R.js - 1) * sy] = p[base + (long)R.js * sy];
+        p[base + (long)(R.je + 1) * sy] = p[base + (long)R.je * sy];
+    } else {
+        const int k = R.ks + a, j = R.js + b;
+        if (k > R.ke) return;
+        const long base = (long)j * sy + k;
+        p[base + (long)(R.is - 1) * sx] = p[base + (long)R.is * sx];
+        p[base + (long)(R.ie + 1) * sx] = p[base + (long)R.ie * sx];
+    }
+}
+
+template <typename real>
+struct ProjectArgs {
+    real* u;
+    real* v;
+    real* w;               // new velocities, corrected in place
+    real* pgu;
+    real* pgv;
+    real* pgw;             // accumulated pressure gradients
+    const real* phi;
+    MuPtrs<real> mu;       // mu_new
+    const double* scal;    // dt, deficit
+    double alpha;
+    int do_correct, do_ghosts, do_pg;
+};
+
+// velo_correction (pllcart3d.c:2133-2227), update_veloghost_points
+// (L2810-2885) and pressure_gradient (L2964-3044) fused: one thread per
+// (i,j,k) of i in [is, ie+1], j in [js, je], k in [ks, ke] of the grid.
+// Ghost copies are written by the thread that owns their source value, after
+// its correction.  grad(phi) at neighbours is evaluated from phi directly
+// (the reference's phi_x/phi_y/phi_z temporaries hold exactly these values).
+template <typename real>
+__global__ void __launch_bounds__(128) k_project(Geo G, Rng Rg, Rng Ru, Rng Rv, Rng Rw, Consts K,
+                                                 ProjectArgs<real> A)
+{
+    const int k = Rg.ks + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = Rg.js + blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = Rg.is + blockIdx.z;
+    if (k > Rg.ke || j > Rg.je) return;
+    const long sx = G.sx, sy = G.sy;
+    const long id = (long)i * sx + (long)j * sy + k;
+    const real* __restrict__ phi = A.phi;
+    const double dt = A.scal[S_DT];
+    const bool inu = (i >= Ru.is) & (i <= Ru.ie) & (j >= Ru.js) & (k >= Ru.ks);
+    const bool inv = (i <= Rv.ie) & (j >= Rv.js) & (k >= Rv.ks);
+    const bool inw = (i <= Rw.ie) & (j >= Rw.js) & (k >= Rw.ks);
+    const bool ghost_i = (i <= Rg.ie);
+
+    if (A.do_correct) {
+        const real fac = (real)(dt * A.alpha / K.Re);
+        real uval = A.u[id], vval = 0, wval = 0;
+        if (ghost_i) {
+            vval = A.v[id];
+            wval = A.w[id];
+        }
+        if (inv) {
+            vval = vval - fac * over_h<real>(phi[id] - phi[id - sy], K.hy, K.ihy, K.pow2);
+            A.v[id] = vval;
+        }
+        if (inw) {
+            wval = wval - fac * over_h<real>(phi[id] - phi[id - 1], K.hz, K.ihz, K.pow2);
+            A.w[id] = wval;
+        }
+        if (inu) {
+            uval = uval - fac * over_h<real>(phi[id] - phi[id - sx], K.hx, K.ihx, K.pow2);
+            A.u[id] = uval;
+        }
+        if (i == Ru.ie + 1 && j >= Ru.js && k >= Ru.ks) {
+            A.u[id] = uval + (real)A.scal[S_DEFICIT];
+        }
+        if (A.do_ghosts && ghost_i) {
+            if (k == Rg.ks) { A.u[id - 1] = uval; A.v[id - 1] = vval; }
+            if (k == Rg.ke) { A.u[id + 1] = uval; A.v[id + 1] = vval; }
+            if (j == Rg.js) { A.u[id - sy] = -uval; A.w[id - sy] = -wval; }
+            if (j == Rg.je) { A.u[id + sy] = -uval; A.w[id + sy] = -wval; }
+            if (i == Rg.is) { A.v[id - sx] = -vval; A.w[id - sx] = -wval; }
+        }
+    } else if (A.do_ghosts && ghost_i) {
+        const real uval = A.u[id], vval = A.v[id], wval = A.w[id];
+        if (k == Rg.ks) { A.u[id - 1] = uval; A.v[id - 1] = vval; }
+        if (k == Rg.ke) { A.u[id + 1] = uval; A.v[id + 1] = vval; }
+        if (j == Rg.js) { A.u[id - sy] = -uval; A.w[id - sy] = -wval; }
+        if (j == Rg.je) { A.u[id + sy] = -uval; A.w[id + sy] = -wval; }
+        if (i == Rg.is) { A.v[id - sx] = -vval; A.w[id - sx] = -wval; }
+    }
+
+    if (A.do_pg) {
+        const real fac = (real)(0.5 * dt * A.alpha);
+        real a, b, c;
+        if (inv) {
+            auto gp = [&](long p) { return over_h<real>(phi[p] - phi[p - sy], K.hy, K.ihy, K.pow2); };
+            const real g0 = gp(id);
+            acoef<VV, 0, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
+            real pxx = a * gp(id - sx) + b * g0 + c * gp(id + sx);
+            acoef<VV, 1, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
+            real pyy = a * gp(id - sy) + b * g0 + c * gp(id + sy);
+            acoef<VV, 2, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
+            real pzz = a * gp(id - 1) + b * g0 + c * gp(id + 1);
+            A.pgv[id] = A.pgv[id] + g0 - fac * (pyy + pxx + pzz);
+        }
+        if (inu) {
+            auto gp = [&](long p) { return over_h<real>(phi[p] - phi[p - sx], K.hx, K.ihx, K.pow2); };
+            const real g0 = gp(id);
+            acoef<VU, 0, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
+            real pxx = a * gp(id - sx) + b * g0 + c * gp(id + sx);
+            acoef<VU, 1, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
+            real pyy = a * gp(id - sy) + b * g0 + c * gp(id + sy);
+            acoef<VU, 2, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
+            real pzz = a * gp(id - 1) + b * g0 + c * gp(id + 1);
+            A.pgu[id] = A.pgu[id] + g0 - fac * (pyy + pxx + pzz);
+        }
+        if (inw) {
+            auto gp = [&](long p) { return over_h<real>(phi[p] - phi[p - 1], K.hz, K.ihz, K.pow2); };
+            const real g0 = gp(id);
+            acoef<VW, 0, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
+            real pxx = a * gp(id - sx) + b * g0 + c * gp(id + sx);
+            acoef<VW, 1, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
+            real pyy = a * gp(id - sy) + b * g0 + c * gp(id + sy);
+            acoef<VW, 2, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
+            real pzz = a * gp(id - 1) + b * g0 + c * gp(id + 1);
+            A.pgw[id] = A.pgw[id] + g0 - fac * (pyy + pxx + pzz);
+        }
+    }
+}
+
+// slope_parameter (pllcart3d.c:722-840) on one rank: bisection for the
+// non-monotonic viscosity law's cm from c along the x line closest to
+// y=0, z=0; also leaves the law's coefficients (L895-900) in the scalars.
+// One thread.
+__global__ void k_slope_parameter(Geo G, Rng R, double Y1, double Z1, double dy, double dz,
+                                  double M, double Mum, double Lambda, double PI,
+                                  const double* __restrict__ cn, double* scal, int* status,
+                                  double* work)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int n = R.ie - R.is + 1;
+    double err = 10.0;
+    int jj = R.js, kk = R.ks;
+    for (int j = R.js; j <= R.je; ++j) {
+        double yc = Y1 - R.js * dy + (dy / 2.0) + j * dy;
+        if (fabs(yc - 0.0) < err) { err = fabs(yc - 0.0); jj = j; }
+    }
+    err = 10.0;
+    for (int k = R.ks; k <= R.ke; ++k) {
+        double zc = Z1 - R.ks * dz + (dz / 2.0) + k * dz;
+        if (fabs(zc - 0.0) < err) { err = fabs(zc - 0.0); kk = k; }
+    }
+    double* croot = work;
+    double* mucell = work + n;
+    for (int i = R.is; i <= R.ie; ++i) croot[i - R.is] = cn[(long)i * G.sx + (long)jj * G.sy + kk];
+    double alpha = exp(M), mum = Mum * alpha;
+    double psi0 = asin(alpha / mum), psi1 = PI - asin(1 / mum);
+    double etam = (PI / 2 - psi0) / (psi1 - psi0);
+    double cL = 0.1, cH = 0.9, cm = 0.5 * (cL + cH), errd = 100, errl = 1e-5;
+    int niter = 0, ok = 1;
+    while (errd > 1e-5) {
+        double a = ((1 - cm) - etam) / ((1 - cm) * (etam - 1));
+        for (int i = 0; i < n; ++i) {
+            double eta = ((1 + a) * croot[i]) / (1 + a * croot[i]);
+            double psi = psi0 * (1 - eta) + psi1 * eta;
+            mucell[i] = mum * sin(psi);
+        }
+        int idx1 = -1, idx2 = -1;
+        for (int i = 0; i < n; ++i) {
+            if (idx1 > 0) break;
+            if (fabs(croot[i]) > errl) idx1 = i;
+        }
+        for (int i = n - 1; i >= 0; --i) {
+            if (idx2 > 0) break;
+            if (fabs(croot[i]) < 1 - errl) idx2 = i;
+        }
+        if (idx1 < 0 || idx2 < 1 || idx1 + 1 >= n) { ok = 0; break; }
+        double mup1 = (mucell[idx1 + 1] - mucell[idx1]) / (croot[idx1 + 1] - croot[idx1]);
+        double mup2 = (mucell[idx2] - mucell[idx2 - 1]) / (croot[idx2] - croot[idx2 - 1]);
+        double lambda = (mup1 + mup2) / (alpha + 1);
+        if (lambda > Lambda) cH = cm;
+        else cL = cm;
+        cm = 0.5 * (cL + cH);
+        errd = fabs(lambda - Lambda);
+        niter++;
+        if (niter > 500) { ok = 0; break; }
+    }
+    if (!ok) atomicOr(status, (int)ST_NOCONV);
+    scal[S_CM] = cm;
+    scal[S_MUM] = mum;
+    scal[S_PSI0] = psi0;
+    scal[S_PSI1] = psi1;
+    scal[S_NMVA] = ((1 - cm) - etam) / ((1 - cm) * (etam - 1));
+}
+
+}  // namespace pll

@@ -1,0 +1,59 @@
+// Shared device-side types for the pllcart3d B200 step.
+//
+// Device layout: every field is one array over the padded box
+// (nx+6) x (ny+2) x (nz+2) in the reference's [i][j][k] order with k
+// contiguous (allocate_3d_calloc.h:46-64), but contiguous in HBM with a row
+// pitch `sy` >= nz+2 (a multiple of 8 elements) and a plane pitch
+// `sx` = (ny+2)*sy.  Index ranges follow grid_setup / simulation_setup for
+// one rank (pllcart3d.c:357-431): interior i in [3, nx+2], j in [1, ny],
+// k in [1, nz]; the u unknowns start at i=4, v at j=2, w at k=2.
+#pragma once
+
+#include <cstdint>
+
+namespace pll {
+
+struct Geo {
+    int nx, ny, nz;   // interior cells
+    int NX, NY, NZ;   // padded logical extents
+    long sx, sy;      // element strides of i and j (k stride is 1)
+    double dx, dy, dz;
+};
+
+struct Rng {
+    int is, ie, js, je, ks, ke;
+};
+
+struct Phys {
+    double Re, Pe, M, Vnorm, Fx, Fy, CFLmax;
+    double Y1, Y2, Z1, Z2;
+    double Mum, PI;
+    int nmvp;
+};
+
+enum Var { VC = 0, VU = 1, VV = 2, VW = 3 };
+
+// device scalar slots (one small array per context)
+enum Scal {
+    S_DT = 0,        // time step of the current step
+    S_VBULK = 1,     // outflow convective speed of the current substep
+    S_DEFICIT = 2,   // inflow - outflow mass-flux deficit per unit area
+    S_CFLMAX = 3,    // max over cells of |u|/dx+|v|/dy+|w|/dz (as bits)
+    S_TIMESTEP = 4,  // Timestep after the diffusive cap
+    S_CM = 5,        // slope parameter of the non-monotonic viscosity law
+    S_QIN = 6,
+    S_QOUT = 7,
+    // 8..11: non-monotonic viscosity coefficients (aux_kernels.cuh)
+    S_TVAL = 12,     // simulated time
+    S_CFLDT = 13,    // CFLmax / max, find_cfl's return value
+    S_COUNT = 16
+};
+
+// sticky status bits
+enum StatusBits {
+    ST_NAN = 1,       // a NaN/Inf met in the CFL scan
+    ST_NOCONV = 2,    // slope-parameter bisection did not converge
+    ST_BOUNDS = 4,    // a kernel's self-check found a bad index
+};
+
+}  // namespace pll

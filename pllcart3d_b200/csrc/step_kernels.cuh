@@ -1,0 +1,533 @@
+// Kernels of the pllcart3d RK3-CN step (pllcart3d.c:156-196), templated on
+// the arithmetic type.  The FP64 instantiation is compiled without
+// multiply-add contraction (--fmad=false) and keeps every division that the
+// reference performs, except divisions by a grid spacing or by 4*ny*nz that
+// is an exact power of two, which are exact multiplications by the exact
+// reciprocal.  Operation order follows the reference expression by
+// expression so that the FP64 path tracks it to rounding level.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace pll {
+
+// ---------------------------------------------------------------------------
+// constants shared by the stencil kernels (host-precomputed, exact as in the
+// reference: each is the same IEEE expression the reference evaluates)
+// ---------------------------------------------------------------------------
+struct Consts {
+    double hx, hy, hz;            // dx, dy, dz
+    double ihx, ihy, ihz;         // 1/dx ... (used only when pow2)
+    double i2hx, i2hy, i2hz;      // 1/(2 dx) ... (used only when pow2)
+    int pow2;                     // all spacings are exact powers of two
+    double cdx, cdy, cdz;         // 1/(Pe h^2), A_conc (pllcart3d.c:1421-1433)
+    double d1x, d1y, d1z;         // 1/(Re h)
+    double d2x, d2y, d2z;         // 2/(Re h)
+    double xuv, xuw;              // 1/(Re dy dx), 1/(Re dz dx)  (Hu_op)
+    double xvu, xvw;              // 1/(Re dx dy), 1/(Re dz dy)  (Hv_op)
+    double xwu, xwv;              // 1/(Re dx dz), 1/(Re dy dz)  (Hw_op)
+    double FxRe, FyRe;            // -(Fx/Re), -(Fy/Re)
+    double Re;
+    double area;                  // (Y2-Y1)*(Z2-Z1)
+    double dx2i;                  // 1/(dx*dx) (phisolver_dct)
+    double CFLmax;
+    double M, Vnorm;
+};
+
+template <typename real>
+__device__ __forceinline__ real over_h(real x, double h, double ih, int pow2)
+{
+    return pow2 ? x * (real)ih : x / (real)h;
+}
+
+// advecting velocity of variable VAR for the pass along AXIS at point id
+// (Hc_op L1563/1591/1621, Hu_op L1669/1696/1722, Hv_op L1780/1807/1834,
+//  Hw_op L1892/1919/1946)
+template <int VAR, int AXIS, typename real>
+__device__ __forceinline__ real adv_vel(const real* __restrict__ self,
+                                       const real* __restrict__ un,
+                                       const real* __restrict__ vn,
+                                       const real* __restrict__ wn, long id,
+                                       long sx, long sy)
+{
+    const real h = (real)0.5, q = (real)0.25;
+    if (VAR == VC) {
+        if (AXIS == 0) return h * (un[id + sx] + un[id]);
+        if (AXIS == 1) return h * (vn[id + sy] + vn[id]);
+        return h * (wn[id + 1] + wn[id]);
+    } else if (VAR == VU) {
+        if (AXIS == 0) return self[id];
+        if (AXIS == 1) return q * (vn[id - sx] + vn[id] + vn[id + sy] + vn[id - sx + sy]);
+        return q * (wn[id - sx] + wn[id] + wn[id + 1] + wn[id - sx + 1]);
+    } else if (VAR == VV) {
+        if (AXIS == 0) return q * (un[id - sy] + un[id + sx - sy] + un[id] + un[id + sx]);
+        if (AXIS == 1) return self[id];
+        return q * (wn[id - sy] + wn[id - sy + 1] + wn[id] + wn[id + 1]);
+    } else {
+        if (AXIS == 0) return q * (un[id - 1] + un[id + sx - 1] + un[id] + un[id + sx]);
+        if (AXIS == 1) return q * (vn[id - 1] + vn[id] + vn[id + sy - 1] + vn[id + sy]);
+        return self[id];
+    }
+}
+
+// WENO5 derivative from five divided differences (calculate_weno,
+// pllcart3d.c:3455-3507)
+template <typename real>
+__device__ __forceinline__ real weno5(real v0, real v1, real v2, real v3, real v4)
+{
+    const real con1 = (real)(1.0 / 6.0), con2 = (real)(13.0 / 12.0), con3 = (real)(1.0 / 4.0);
+    real maxd = (real)0, sq;
+    sq = v0 * v0; maxd = (maxd > sq) ? maxd : sq;
+    sq = v1 * v1; maxd = (maxd > sq) ? maxd : sq;
+    sq = v2 * v2; maxd = (maxd > sq) ? maxd : sq;
+    sq = v3 * v3; maxd = (maxd > sq) ? maxd : sq;
+    sq = v4 * v4; maxd = (maxd > sq) ? maxd : sq;
+    real c1 = con1 * ((real)2.0 * v0 - (real)7.0 * v1 + (real)11.0 * v2);
+    real c2 = con1 * ((real)-1.0 * v1 + (real)5.0 * v2 + (real)2.0 * v3);
+    real c3 = con1 * ((real)2.0 * v2 + (real)5.0 * v3 - (real)1.0 * v4);
+    real t1 = v0 - (real)2.0 * v1 + (real)1.0 * v2;
+    real t2 = v0 - (real)4.0 * v1 + (real)3.0 * v2;
+    real s1 = (con2 * t1 * t1) + (con3 * t2 * t2);
+    t1 = v1 - (real)2.0 * v2 + v3;
+    t2 = v1 - v3;
+    real s2 = (con2 * t1 * t1) + (con3 * t2 * t2);
+    t1 = (real)1.0 * v2 - (real)2.0 * v3 + v4;
+    t2 = (real)3.0 * v2 - (real)4.0 * v3 + v4;
+    real s3 = (con2 * t1 * t1) + (con3 * t2 * t2);
+    real eps = (real)1.0e-6 * maxd + (real)1.0e-99;
+    real a1 = (real)0.1 / ((s1 + eps) * (s1 + eps));
+    real a2 = (real)0.6 / ((s2 + eps) * (s2 + eps));
+    real a3 = (real)0.3 / ((s3 + eps) * (s3 + eps));
+    real at = a1 + a2 + a3;
+    return (a1 / at) * c1 + (a2 / at) * c2 + (a3 / at) * c3;
+}
+
+// D2 value an earlier directional pass of the same H*_op call left in its
+// scratch line at index m (pllcart3d.c:1545-1546: D1/D2 are allocated once
+// per call, zeroed, and reused by the x, y and z passes; each pass writes
+// D2 only on the variable's own range, so the ENO-2 closure reads one point
+// outside the range pick up the previous pass's last line).  The x pass
+// leaves (j=je, k=ke), the y pass (i=ie, k=ke).
+template <typename real>
+__device__ real stale_d2(const real* __restrict__ q, const Geo& G, const Rng& R,
+                         const Consts& K, int pass, int m)
+{
+    for (int p = pass - 1; p >= 0; --p) {
+        int s = p == 0 ? R.is : R.js, e = p == 0 ? R.ie : R.je;
+        if (m >= s && m <= e) {
+            long base, st;
+            double h, ih, i2h;
+            if (p == 0) {
+                base = (long)R.je * G.sy + R.ke; st = G.sx; h = K.hx; ih = K.ihx; i2h = K.i2hx;
+            } else {
+                base = (long)R.ie * G.sx + R.ke; st = G.sy; h = K.hy; ih = K.ihy; i2h = K.i2hy;
+            }
+            real d1m = over_h<real>(q[base + (long)(m + 1) * st] - q[base + (long)m * st], h, ih, K.pow2);
+            real d1p = over_h<real>(q[base + (long)m * st] - q[base + (long)(m - 1) * st], h, ih, K.pow2);
+            return K.pow2 ? (d1m - d1p) * (real)i2h : (d1m - d1p) / ((real)2.0 * (real)h);
+        }
+    }
+    return (real)0;
+}
+
+// upwind derivative of q along AXIS at point id (line position m); the
+// ENO-2 closure on the first and last two points of the range, WENO5
+// elsewhere (e.g. Hc_op pllcart3d.c:1553-1576)
+template <int AXIS, typename real>
+__device__ __forceinline__ real upwind_deriv(const real* __restrict__ q, const Geo& G,
+                                             const Rng& R, const Consts& K, long id,
+                                             int m, real vv)
+{
+    const int s = AXIS == 0 ? R.is : AXIS == 1 ? R.js : R.ks;
+    const int e = AXIS == 0 ? R.ie : AXIS == 1 ? R.je : R.ke;
+    const long st = AXIS == 0 ? G.sx : AXIS == 1 ? G.sy : 1;
+    const double h = AXIS == 0 ? K.hx : AXIS == 1 ? K.hy : K.hz;
+    const double ih = AXIS == 0 ? K.ihx : AXIS == 1 ? K.ihy : K.ihz;
+    const double i2h = AXIS == 0 ? K.i2hx : AXIS == 1 ? K.i2hy : K.i2hz;
+    const int sign = (vv >= (real)0) ? 1 : -1;
+    if ((m <= s + 1) | (m >= e - 1)) {
+        const int kk = (sign == 1) ? m - 1 : m;
+        const long b = id + (long)(kk - m) * st;
+        real d1k = over_h<real>(q[b + st] - q[b], h, ih, K.pow2);
+        real d2a, d2b;
+        if (kk >= s) {
+            real d1m = over_h<real>(q[b] - q[b - st], h, ih, K.pow2);
+            d2a = K.pow2 ? (d1k - d1m) * (real)i2h : (d1k - d1m) / ((real)2.0 * (real)h);
+        } else {
+            d2a = stale_d2<real>(q, G, R, K, AXIS, kk);
+        }
+        if (kk + 1 <= e) {
+            real d1p = over_h<real>(q[b + 2 * st] - q[b + st], h, ih, K.pow2);
+            d2b = K.pow2 ? (d1p - d1k) * (real)i2h : (d1p - d1k) / ((real)2.0 * (real)h);
+        } else {
+            d2b = stale_d2<real>(q, G, R, K, AXIS, kk + 1);
+        }
+        real d2v = (fabs(d2a) <= fabs(d2b)) ? d2a : d2b;
+        return d1k + d2v * (real)h * (real)sign;
+    }
+    // WENO: D1[kk + sign*t], t = 0..4, kk = m-3 (sign>0) or m+2 (sign<0)
+    const int kk = m - 3 - (int)(2.5 * (sign - 1));
+    real v[5];
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+        const long p = id + (long)(kk + sign * t - m) * st;
+        v[t] = over_h<real>(q[p + st] - q[p], h, ih, K.pow2);
+    }
+    return weno5<real>(v[0], v[1], v[2], v[3], v[4]);
+}
+
+// implicit-operator coefficients (A_conc/A_umom/A_vmom/A_wmom,
+// pllcart3d.c:1411-1536) from the viscosity arrays
+template <int VAR, int AXIS, typename real>
+__device__ __forceinline__ void acoef(const Consts& K, const Geo& G,
+                                      const real* __restrict__ mc,
+                                      const real* __restrict__ mxy,
+                                      const real* __restrict__ mxz,
+                                      const real* __restrict__ myz, long id,
+                                      real& a, real& b, real& c)
+{
+    const long sx = G.sx, sy = G.sy;
+    if (VAR == VC) {
+        const real d = (real)(AXIS == 0 ? K.cdx : AXIS == 1 ? K.cdy : K.cdz);
+        a = d;
+        c = d;
+    } else if (VAR == VU) {
+        if (AXIS == 0) {
+            a = over_h<real>((real)K.d2x * mc[id - sx], K.hx, K.ihx, K.pow2);
+            c = over_h<real>((real)K.d2x * mc[id], K.hx, K.ihx, K.pow2);
+        } else if (AXIS == 1) {
+            a = over_h<real>((real)K.d1y * mxy[id], K.hy, K.ihy, K.pow2);
+            c = over_h<real>((real)K.d1y * mxy[id + sy], K.hy, K.ihy, K.pow2);
+        } else {
+            a = over_h<real>((real)K.d1z * mxz[id], K.hz, K.ihz, K.pow2);
+            c = over_h<real>((real)K.d1z * mxz[id + 1], K.hz, K.ihz, K.pow2);
+        }
+    } else if (VAR == VV) {
+        if (AXIS == 0) {
+            a = over_h<real>((real)K.d1x * mxy[id], K.hx, K.ihx, K.pow2);
+            c = over_h<real>((real)K.d1x * mxy[id + sx], K.hx, K.ihx, K.pow2);
+        } else if (AXIS == 1) {
+            a = over_h<real>((real)K.d2y * mc[id - sy], K.hy, K.ihy, K.pow2);
+            c = over_h<real>((real)K.d2y * mc[id], K.hy, K.ihy, K.pow2);
+        } else {
+            a = over_h<real>((real)K.d1z * myz[id], K.hz, K.ihz, K.pow2);
+            c = over_h<real>((real)K.d1z * myz[id + 1], K.hz, K.ihz, K.pow2);
+        }
+    } else {
+        if (AXIS == 0) {
+            a = over_h<real>((real)K.d1x * mxz[id], K.hx, K.ihx, K.pow2);
+            c = over_h<real>((real)K.d1x * mxz[id + sx], K.hx, K.ihx, K.pow2);
+        } else if (AXIS == 1) {
+            a = over_h<real>((real)K.d1y * myz[id], K.hy, K.ihy, K.pow2);
+            c = over_h<real>((real)K.d1y * myz[id + sy], K.hy, K.ihy, K.pow2);
+        } else {
+            a = over_h<real>((real)K.d2z * mc[id - 1], K.hz, K.ihz, K.pow2);
+            c = over_h<real>((real)K.d2z * mc[id], K.hz, K.ihz, K.pow2);
+        }
+    }
+    b = -(a + c);
+}
+
+template <typename real>
+struct MuPtrs {
+    const real* cell;
+    const real* xy;
+    const real* xz;
+    const real* yz;
+};
+
+template <typename real>
+struct ExplicitArgs {
+    const real* q;      // q_old of the variable
+    const real* un;     // advecting / cross-term velocities
+    const real* vn;
+    const real* wn;
+    MuPtrs<real> mu;    // mu_old
+    const real* cn;     // c_new (body force of u and v)
+    const real* pg;     // accumulated pressure gradient of the variable
+    const real* Hm;     // explicit term of the previous substep
+    real* H;            // explicit term of this substep (out)
+    real* S;            // right-hand side of the ADI solve (out)
+    const double* scal; // device scalars (dt)
+    double g, r, alpha; // RK3 gamma, rho and gamma+rho
+};
+
+// ---------------------------------------------------------------------------
+// explicit operator + right-hand side of one variable
+// Hc_op/Hu_op/Hv_op/Hw_op (pllcart3d.c:1539-1980) fused with the source
+// assembly of concentration/xmom/ymom/zmom (L573-590, L970-989, L1127-1146,
+// L1280-1298)
+// ---------------------------------------------------------------------------
+template <int VAR, typename real>
+__global__ void __launch_bounds__(128) k_explicit(Geo G, Rng R, Consts K,
+                                                  ExplicitArgs<real> A)
+{
+    const int k = R.ks + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = R.js + blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = R.is + blockIdx.z;
+    if (k > R.ke || j > R.je) return;
+    const long sx = G.sx, sy = G.sy;
+    const long id = (long)i * sx + (long)j * sy + k;
+    const real* __restrict__ q = A.q;
+
+    real vx = adv_vel<VAR, 0, real>(q, A.un, A.vn, A.wn, id, sx, sy);
+    real cx = vx * upwind_deriv<0, real>(q, G, R, K, id, i, vx);
+    real vy = adv_vel<VAR, 1, real>(q, A.un, A.vn, A.wn, id, sx, sy);
+    real cy = vy * upwind_deriv<1, real>(q, G, R, K, id, j, vy);
+    real vz = adv_vel<VAR, 2, real>(q, A.un, A.vn, A.wn, id, sx, sy);
+    real cz = vz * upwind_deriv<2, real>(q, G, R, K, id, k, vz);
+    real ct = cz + cx + cy;
+    real H;
+    if (VAR == VC) {
+        H = -(ct);
+    } else {
+        const real* __restrict__ un = A.un;
+        const real* __restrict__ vn = A.vn;
+        const real* __restrict__ wn = A.wn;
+        real s1, s2, s3, s4;
+        if (VAR == VU) {
+            s1 = (real)K.xuv * A.mu.xy[id + sy] * (vn[id + sy] - vn[id - sx + sy]);
+            s2 = (real)K.xuv * A.mu.xy[id] * (vn[id] - vn[id - sx]);
+            s3 = (real)K.xuw * A.mu.xz[id + 1] * (wn[id + 1] - wn[id - sx + 1]);
+            s4 = (real)K.xuw * A.mu.xz[id] * (wn[id] - wn[id - sx]);
+        } else if (VAR == VV) {
+            s1 = (real)K.xvu * A.mu.xy[id + sx] * (un[id + sx] - un[id + sx - sy]);
+            s2 = (real)K.xvu * A.mu.xy[id] * (un[id] - un[id - sy]);
+            s3 = (real)K.xvw * A.mu.yz[id + 1] * (wn[id + 1] - wn[id - sy + 1]);
+            s4 = (real)K.xvw * A.mu.yz[id] * (wn[id] - wn[id - sy]);
+        } else {
+            s1 = (real)K.xwu * A.mu.xz[id + sx] * (un[id + sx] - un[id + sx - 1]);
+            s2 = (real)K.xwu * A.mu.xz[id] * (un[id] - un[id - 1]);
+            s3 = (real)K.xwv * A.mu.yz[id + sy] * (vn[id + sy] - vn[id + sy - 1]);
+            s4 = (real)K.xwv * A.mu.yz[id] * (vn[id] - vn[id - 1]);
+        }
+        H = -ct + s1 - s2 + s3 - s4;
+    }
+    A.H[id] = H;
+
+    // right-hand side dt*(gamma H + rho H_old + alpha A q_old + alpha body)
+    const real dt = (real)A.scal[S_DT];
+    const real alpha = (real)A.alpha;
+    real conv = ((real)A.g * H + (real)A.r * A.Hm[id]);
+    real a, b, c;
+    acoef<VAR, 0, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
+    real ax = a * q[id - sx] + b * q[id] + c * q[id + sx];
+    acoef<VAR, 1, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
+    real ay = a * q[id - sy] + b * q[id] + c * q[id + sy];
+    acoef<VAR, 2, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
+    real az = a * q[id - 1] + b * q[id] + c * q[id + 1];
+    real diff = alpha * (ax + ay + az);
+    real S;
+    if (VAR == VC) {
+        S = dt * (conv + diff);
+    } else {
+        real bf;
+        if (VAR == VU) {
+            real cval = (real)0.5 * (A.cn[id] + A.cn[id - sx]);
+            bf = alpha * ((real)K.FxRe * cval - (A.pg[id] / (real)K.Re));
+        } else if (VAR == VV) {
+            real cval = (real)0.5 * (A.cn[id] + A.cn[id - sy]);
+            bf = alpha * ((real)K.FyRe * cval - (A.pg[id] / (real)K.Re));
+        } else {
+            bf = alpha * (-(A.pg[id] / (real)K.Re));
+        }
+        S = dt * (conv + diff + bf);
+    }
+    A.S[id] = S;
+}
+
+// closure codes of the first/last unknown of an ADI line:
+// 1 b+=a (Neumann / symmetry), 2 b-=a (reflection about a wall face),
+// 3 rhs-=a*0 (Dirichlet wall face), 0 none
+template <int VAR, int AXIS>
+struct Closure {
+    // x: c L675, u L1075, v L1231, w L1378 ; y: c L610, u L1010, v L1167,
+    // w L1317 ; z: c L640, u L1039, v L1196, w L1344
+    static constexpr int lo = AXIS == 0 ? (VAR <= VU ? 3 : 2)
+                            : AXIS == 1 ? (VAR == VC ? 1 : VAR == VV ? 3 : 2)
+                                        : (VAR == VW ? 3 : 1);
+    static constexpr int hi = AXIS == 0 ? 0 : lo;
+};
+
+// ---------------------------------------------------------------------------
+// ADI line solve along y or z: (1 - fac A) x = S, serial Thomas as
+// tridiag_1rhs (pllcart3d.c:3511-3536); one thread per line; the eliminated
+// c' goes to scratch `cc`, the eliminated rhs overwrites S in place
+// (concentration L592-650, xmom L991-1049, ymom L1148-1206, zmom L1300-1354)
+// ---------------------------------------------------------------------------
+template <int VAR, int AXIS, typename real>
+__global__ void __launch_bounds__(128) k_adi_yz(Geo G, Rng R, Consts K, MuPtrs<real> mu,
+                                                real* __restrict__ S, real* __restrict__ cc,
+                                                const double* __restrict__ scal, double alpha)
+{
+    // line index: AXIS==1 -> (i, k); AXIS==2 -> (i, j)
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = R.is + blockIdx.y;
+    int j, k;
+    long st;
+    int n;
+    if (AXIS == 1) {
+        k = R.ks + t;
+        if (k > R.ke) return;
+        j = R.js;
+        st = G.sy;
+        n = R.je - R.js + 1;
+    } else {
+        j = R.js + t;
+        if (j > R.je) return;
+        k = R.ks;
+        st = 1;
+        n = R.ke - R.ks + 1;
+    }
+    const real fac = (real)(0.5 * scal[S_DT] * alpha);
+    const long base = (long)i * G.sx + (long)j * G.sy + k;
+    constexpr int LO = Closure<VAR, AXIS>::lo, HI = Closure<VAR, AXIS>::hi;
+    real cprev = 0, rprev = 0;
+    for (int m = 0; m < n; ++m) {
+        const long id = base + (long)m * st;
+        real a, b, c;
+        acoef<VAR, AXIS, real>(K, G, mu.cell, mu.xy, mu.xz, mu.yz, id, a, b, c);
+        real la = -fac * a, lb = (real)1.0 - fac * b, lc = -fac * c, lr = S[id];
+        if (m == 0) {
+            if (LO == 1) lb += la;
+            else if (LO == 2) lb -= la;
+            else if (LO == 3) lr -= la * (real)0.0;
+        }
+        if (m == n - 1) {
+            if (HI == 1) lb += lc;
+            else if (HI == 2) lb -= lc;
+            else if (HI == 3) lr -= lc * (real)0.0;
+        }
+        real bb, cm, rm;
+        if (m == 0) {
+            bb = lb;
+            cm = lc / bb;
+            rm = lr / bb;
+        } else {
+            bb = lb - cprev * la;
+            cm = lc / bb;
+            rm = (lr - rprev * la) / bb;
+        }
+        cc[id] = cm;
+        S[id] = rm;
+        cprev = cm;
+        rprev = rm;
+    }
+    real xnext = rprev;
+    for (int m = n - 2; m >= 0; --m) {
+        const long id = base + (long)m * st;
+        real x = S[id] - xnext * cc[id];
+        S[id] = x;
+        xnext = x;
+    }
+}
+
+template <typename real>
+struct XsweepArgs {
+    MuPtrs<real> mu;     // mu_new
+    const real* q;       // q_old
+    real* qn;            // q_new (out)
+    real* H;             // explicit term (outflow plane written here)
+    const real* Hm;      // previous explicit term
+    real* S;             // eliminated rhs from the y/z sweeps (scratch)
+    real* cc;            // scratch
+    const double* scal;  // dt, vbulk
+    double g, r, alpha;
+};
+
+// ---------------------------------------------------------------------------
+// ADI line solve along x with pll_tridiag's one-rank arithmetic
+// (pll_tridiag.c:21-47, 96-110), the convective outflow closure
+// (e.g. pllcart3d.c:677-683), new = old + delta, and for c the Neumann
+// ghost copies of pllcart3d.c:700-712.  One thread per (j,k) line.
+// ---------------------------------------------------------------------------
+template <int VAR, typename real>
+__global__ void __launch_bounds__(128) k_adi_x(Geo G, Rng R, Consts K, XsweepArgs<real> A)
+{
+    const int k = R.ks + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = R.js + blockIdx.y;
+    if (k > R.ke) return;
+    const long sx = G.sx;
+    const int n = R.ie - R.is + 1;
+    const real dt = (real)A.scal[S_DT];
+    const real fac = (real)(0.5 * A.scal[S_DT] * A.alpha);
+    const real vbulk = (real)A.scal[S_VBULK];
+    const long base = (long)R.is * sx + (long)j * G.sy + k;
+    const long rb = base + (long)n * sx;
+    constexpr int LO = Closure<VAR, 0>::lo;
+    // outflow plane, explicit convective boundary condition
+    real Hb = -vbulk * (A.q[rb] - A.q[rb - sx]);
+    Hb = over_h<real>(Hb, K.hx, K.ihx, K.pow2);
+    A.H[rb] = Hb;
+    const real boun = dt * ((real)A.g * Hb + (real)A.r * A.Hm[rb]);
+    A.qn[rb] = A.q[rb] + boun;
+
+    real cprev = 0, rprev = 0;
+    for (int m = 0; m < n; ++m) {
+        const long id = base + (long)m * sx;
+        real a, b, c;
+        acoef<VAR, 0, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
+        real la = -fac * a, lb = (real)1.0 - fac * b, lc = -fac * c, lr = A.S[id];
+        if (m == 0) {
+            if (LO == 2) lb -= la;
+            else if (LO == 3) lr -= la * (real)0.0;
+        }
+        if (m == n - 1) lr -= lc * boun;
+        real cm, rm;
+        if (m == 0) {
+            lb = lb - (real)0.0 * la;
+            cm = lc / lb;
+            rm = (lr - (real)0.0 * la) / lb;
+        } else {
+            lb = (lb - cprev * la);
+            cm = lc / lb;
+            rm = (lr - rprev * la) / lb;
+        }
+        A.cc[id] = cm;
+        A.S[id] = rm;
+        cprev = cm;
+        rprev = rm;
+    }
+    // back substitution, q_new = q_old + delta
+    real xnext = rprev - cprev * (real)0.0;
+    {
+        const long id = base + (long)(n - 1) * sx;
+        A.qn[id] = A.q[id] + xnext;
+    }
+    for (int m = n - 2; m >= 0; --m) {
+        const long id = base + (long)m * sx;
+        real x = A.S[id] - A.cc[id] * xnext;
+        A.qn[id] = A.q[id] + x;
+        xnext = x;
+    }
+    if (VAR == VC) {
+        // Neumann ghosts in y (pllcart3d.c:700-705) then z (L707-712); the
+        // z copies run over j in [js-1, je+1] so the corners copy the y
+        // ghosts, which equal this line's values
+        const long sy = G.sy;
+        const bool jlo = (j == R.js), jhi = (j == R.je);
+        const bool klo = (k == R.ks), khi = (k == R.ke);
+        if (jlo | jhi | klo | khi) {
+            for (int m = 0; m < n; ++m) {
+                const long id = base + (long)m * sx;
+                const real v = A.qn[id];
+                if (jlo) A.qn[id - sy] = v;
+                if (jhi) A.qn[id + sy] = v;
+                if (klo) {
+                    A.qn[id - 1] = v;
+                    if (jlo) A.qn[id - sy - 1] = v;
+                    if (jhi) A.qn[id + sy - 1] = v;
+                }
+                if (khi) {
+                    A.qn[id + 1] = v;
+                    if (jlo) A.qn[id - sy + 1] = v;
+                    if (jhi) A.qn[id + sy + 1] = v;
+                }
+            }
+        }
+    }
+}
+
+}  // namespace pll

@@ -1,0 +1,207 @@
+"""Host-side front end of the GPU step: the reference's step routines as
+methods of a resident-state solver.
+
+``Solver`` owns one ``pllgpu_ctx`` (device state in HBM).  Its methods carry
+the names of the reference routines they replace (pllcart3d.c) and run them
+on the GPU against the resident state; ``step(n)`` runs whole time steps
+(pllcart3d.c:158-195) as CUDA-graph replays.  Fields are numpy float64
+arrays over the padded box ``(nx+6, ny+2, nz+2)`` in the reference's
+``[i][j][k]`` order.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .params import Params
+
+RK1 = (8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0)   # global_variables.h:17
+RK2 = (0.0, -17.0 / 60.0, -5.0 / 12.0)      # global_variables.h:18
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Solver:
+    def __init__(self, params: Params, device: int = 0, exact_dct: bool = True,
+                 use_graph: bool = True):
+        params.validate()
+        self.params = params
+        L = _lib.lib()
+        p = _lib.Params()
+        p.nx, p.ny, p.nz = params.nx, params.ny, params.nz
+        p.nmvp = params.Nmvp
+        p.X1, p.X2, p.Y1, p.Y2, p.Z1, p.Z2 = (params.X1, params.X2, params.Y1,
+                                              params.Y2, params.Z1, params.Z2)
+        p.Re, p.Pe, p.Vratio = params.Re, params.Pe, params.Vratio
+        p.Fx, p.Fy, p.CFLmax = params.Fx, params.Fy, params.CFLmax
+        p.Timestep, p.Mum, p.Lambda = params.Timestep, params.Mum, params.Lambda
+        p.precision = 0
+        p.exact_dct = int(bool(exact_dct))
+        p.use_graph = int(bool(use_graph))
+        self._L = L
+        self._h = L.pllgpu_create(ctypes.byref(p), int(device))
+        if not self._h:
+            raise _lib.PllGpuError(2, "pllgpu_create")
+        self.shape = params.shape
+
+    # ---- lifetime ---------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._L.pllgpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, code: int, what: str) -> None:
+        if code != 0:
+            raise _lib.PllGpuError(code, what)
+
+    # ---- state ------------------------------------------------------------
+    def set(self, name: str, arr: np.ndarray) -> None:
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.shape != self.shape:
+            raise ValueError(f"{name}: shape {a.shape} != {self.shape}")
+        fid = _lib.FIELD_NAMES.index(name)
+        self._check(self._L.pllgpu_set_field(self._h, fid, _dp(a)), f"set {name}")
+
+    def get(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.float64)
+        fid = _lib.FIELD_NAMES.index(name)
+        self._check(self._L.pllgpu_get_field(self._h, fid, _dp(out)), f"get {name}")
+        return out
+
+    def state(self, names=None) -> dict:
+        return {n: self.get(n) for n in (names or _lib.FIELD_NAMES)}
+
+    def load_ic(self, ic: dict) -> None:
+        """Initial fields into the *_new arrays, then the start-up of
+        pllcart3d.c:81-83 and 126-154."""
+        for k in "cuvw":
+            self.set(f"{k}_new", ic[k])
+        self._check(self._L.pllgpu_start(self._h), "start")
+
+    # ---- time stepping ----------------------------------------------------
+    def step(self, n: int = 1) -> None:
+        self._check(self._L.pllgpu_steps(self._h, int(n)), "steps")
+
+    @property
+    def dt(self) -> float:
+        return self._L.pllgpu_last_dt(self._h)
+
+    @property
+    def timestep(self) -> float:
+        return self._L.pllgpu_timestep(self._h)
+
+    @property
+    def tval(self) -> float:
+        return self._L.pllgpu_tval(self._h)
+
+    @property
+    def kernels_per_step(self) -> int:
+        return self._L.pllgpu_kernels_per_step(self._h)
+
+    def status(self) -> int:
+        return self._L.pllgpu_status(self._h)
+
+    def clear_status(self) -> None:
+        self._L.pllgpu_clear_status(self._h)
+
+    # ---- reference routines, one at a time ---------------------------------
+    def _routine(self, name: str, *scal) -> float:
+        vin = (ctypes.c_double * 4)(*(list(scal) + [0.0] * (4 - len(scal))))
+        vout = (ctypes.c_double * 4)()
+        self._check(self._L.pllgpu_routine(self._h, _lib.ROUTINES[name], vin, vout), name)
+        return vout[0]
+
+    def concentration(self, dt, g, r, vbulk):
+        """pllcart3d.c:555-719 (advecting velocities: u/v/w_new)."""
+        self._routine("concentration", dt, g, r, vbulk)
+
+    def calculate_viscosity(self):
+        """pllcart3d.c:843-886 of c_new into mu_new (889-948 when Nmvp=1)."""
+        self._routine("viscosity_new")
+
+    def xmom(self, dt, g, r, vbulk):
+        self._routine("xmom", dt, g, r, vbulk)
+
+    def ymom(self, dt, g, r, vbulk):
+        self._routine("ymom", dt, g, r, vbulk)
+
+    def zmom(self, dt, g, r, vbulk):
+        self._routine("zmom", dt, g, r, vbulk)
+
+    def update_velo_boundary(self):
+        self._routine("velo_ghosts")
+
+    update_veloghost_points = update_velo_boundary
+
+    def divergence(self):
+        self._routine("divergence")
+
+    def phisolver_dct(self, dt, g, r):
+        self._routine("phisolver", dt, g, r)
+
+    def update_phi_ghosts(self):
+        self._routine("phi_ghosts")
+
+    def velo_correction(self, dt, g, r):
+        self._routine("velo_correction", dt, g, r)
+
+    def pressure_gradient(self, dt, g, r):
+        self._routine("pressure_gradient", dt, g, r)
+
+    def update_old(self):
+        """update_old_conc / update_old_velo / update_old_visc."""
+        self._routine("rotate")
+
+    def bulk_velo(self) -> float:
+        return self._routine("bulk_velo")
+
+    def find_cfl(self) -> float:
+        return self._routine("find_cfl")
+
+    def substep(self, dt, rk):
+        self._routine("substep", dt, float(rk))
+
+
+def tridiag_batch(a, b, c, r):
+    """pll_tridiag (pll_tridiag.c:152) on the GPU for N systems of length n
+    (arrays shaped (N, n)); returns (b, c, r) as the reference leaves them."""
+    L = _lib.lib()
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.array(b, dtype=np.float64, order="C")
+    c = np.array(c, dtype=np.float64, order="C")
+    r = np.array(r, dtype=np.float64, order="C")
+    N, n = a.shape
+    code = L.pllgpu_tridiag_batch(N, n, _dp(a), _dp(b), _dp(c), _dp(r))
+    if code:
+        raise _lib.PllGpuError(code, "tridiag_batch")
+    return b, c, r
+
+
+def dct2d_batch(kind: int, x: np.ndarray) -> np.ndarray:
+    """FFTW REDFT10 (kind 0) / REDFT01 (kind 1) over the last two axes."""
+    L = _lib.lib()
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    howmany = int(np.prod(x.shape[:-2])) if x.ndim > 2 else 1
+    n0, n1 = x.shape[-2:]
+    out = np.empty_like(x)
+    code = L.pllgpu_dct2d_batch(int(kind), n0, n1, howmany, _dp(x), _dp(out))
+    if code:
+        raise _lib.PllGpuError(code, "dct2d_batch")
+    return out

@@ -1,0 +1,172 @@
+"""GPU step against the CPU restatement (oracle/), through the pllgpu_ C ABI.
+
+Tolerance: relative max-norm 1e-10 per field (max|gpu-cpu| / max|cpu|), the
+bar the FP64 form is held to; the FP64 kernels keep the reference's
+operation order without multiply-add contraction, so the observed error is
+set by exp() rounding differences between CUDA and glibc.
+"""
+
+import numpy as np
+import pytest
+
+from oracle.pyref import FIELDS, OracleRun
+from pllcart3d_b200.ic import workload_fields
+from pllcart3d_b200.params import workload
+from tests.util import STATE_FIELDS, rel_maxnorm
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def _solver(params, **kw):
+    from pllcart3d_b200.solver import Solver
+
+    return Solver(params, **kw)
+
+
+def _pair(name, warm_steps=1, **kw):
+    wl = workload(name)
+    wl.params = wl.params.replace(**kw)
+    ic = workload_fields(wl)
+    o = OracleRun(wl.params, ic)
+    o.steps(warm_steps)
+    s = _solver(wl.params)
+    s.load_ic(ic)
+    for f in FIELDS:
+        s.set(f, o.get(f))
+    return wl, o, s
+
+
+def _cmp(s, o, names, tol=TOL):
+    worst = {}
+    for f in names:
+        e = rel_maxnorm(s.get(f), o.get(f))
+        worst[f] = e
+        assert e <= tol, f"{f}: rel err {e:.3e} > {tol}"
+    return worst
+
+
+@pytest.mark.parametrize("name,kw", [
+    ("fingering-16x8x8", {}),
+    ("fingering-20x6x9", {"Fx": 2.0, "Fy": -1.0}),
+])
+def test_routines_one_by_one(name, kw):
+    wl, o, s = _pair(name, warm_steps=2, **kw)
+    dt, g, r = o.step_dt(), 5.0 / 12.0, -17.0 / 60.0
+    vb = o.bulk_velo()
+    assert s.bulk_velo() == vb
+    assert s.find_cfl() == pytest.approx(o.find_cfl(), rel=1e-15)
+    o.call("concentration", dt, g, r, vb); s.concentration(dt, g, r, vb)
+    _cmp(s, o, ["c_new", "c_hn"])
+    o.call("viscosity_new"); s.calculate_viscosity()
+    _cmp(s, o, ["mu_new_cell", "mu_new_xy", "mu_new_xz", "mu_new_yz"], 1e-14)
+    for v, fn in (("u", "xmom"), ("v", "ymom"), ("w", "zmom")):
+        o.call(fn, dt, g, r, vb); getattr(s, fn)(dt, g, r, vb)
+        _cmp(s, o, [f"{v}_new", f"{v}_hn"])
+    o.call("velo_ghosts"); s.update_velo_boundary()
+    _cmp(s, o, ["u_new", "v_new", "w_new"])
+    o.call("divergence"); s.divergence()
+    _cmp(s, o, ["div"])
+    o.call("phisolver", dt, g, r); s.phisolver_dct(dt, g, r)
+    _cmp(s, o, ["phi"])
+    o.call("phi_ghosts"); s.update_phi_ghosts()
+    _cmp(s, o, ["phi"])
+    o.call("velo_correction", dt, g, r); s.velo_correction(dt, g, r)
+    _cmp(s, o, ["u_new", "v_new", "w_new"])
+    o.call("velo_ghosts"); s.update_veloghost_points()
+    o.call("pressure_gradient", dt, g, r); s.pressure_gradient(dt, g, r)
+    _cmp(s, o, ["u_new", "v_new", "w_new", "u_pg", "v_pg", "w_pg"])
+    o.call("rotate"); s.update_old()
+    _cmp(s, o, FIELDS)
+
+
+def test_routines_without_exp_are_bitwise():
+    """Stages that do not call exp() reproduce the restatement exactly."""
+    wl, o, s = _pair("fingering-16x8x8", warm_steps=3)
+    dt, g, r = o.step_dt(), 8.0 / 15.0, 0.0
+    vb = o.bulk_velo()
+    o.call("concentration", dt, g, r, vb); s.concentration(dt, g, r, vb)
+    for f in ("c_new", "c_hn"):
+        assert np.array_equal(s.get(f), o.get(f)), f
+    o.call("divergence"); s.divergence()
+    o.call("phisolver", dt, g, r); s.phisolver_dct(dt, g, r)
+    assert np.array_equal(s.get("phi"), o.get("phi"))
+
+
+@pytest.mark.parametrize("name,steps,kw", [
+    ("fingering-64x32x32", 200, {}),
+    ("fingering-20x6x9", 30, {"Fx": 1.0, "Fy": 2.0}),
+    ("fingering-18x9x7", 20, {"Nmvp": 1, "Vratio": 1.0}),
+])
+def test_full_steps_match_oracle(name, steps, kw):
+    wl = workload(name)
+    wl.params = wl.params.replace(**kw)
+    ic = workload_fields(wl)
+    o = OracleRun(wl.params, ic)
+    s = _solver(wl.params)
+    s.load_ic(ic)
+    s.step(steps)
+    o.steps(steps)
+    assert s.dt == pytest.approx(o.dt, rel=1e-12)
+    _cmp(s, o, STATE_FIELDS)
+
+
+def test_graph_and_stream_paths_agree():
+    wl = workload("fingering-16x8x8")
+    ic = workload_fields(wl)
+    a = _solver(wl.params, use_graph=True)
+    b = _solver(wl.params, use_graph=False)
+    a.load_ic(ic); b.load_ic(ic)
+    a.step(7); b.step(7)
+    for f in STATE_FIELDS:
+        assert np.array_equal(a.get(f), b.get(f)), f
+
+
+def test_nan_is_reported_not_trapped():
+    from pllcart3d_b200._lib import PllGpuError
+
+    wl = workload("fingering-16x8x8")
+    ic = workload_fields(wl)
+    ic["u"][8, 4, 4] = np.nan
+    s = _solver(wl.params)
+    s.load_ic(ic)
+    with pytest.raises(PllGpuError) as e:
+        s.step(1)
+    assert e.value.code == 1
+    s.clear_status()
+    assert s.status() == 0
+
+
+def test_tridiag_and_dct_primitives():
+    import ctypes
+
+    from oracle.pyref import ORACLE_LIB
+    from pllcart3d_b200.solver import dct2d_batch, tridiag_batch
+
+    P = ctypes.POINTER(ctypes.c_double)
+    L = ctypes.CDLL(ORACLE_LIB)
+    L.orc_thomas_pll.argtypes = [ctypes.c_int, P, P, P, P]
+    L.pll_dct_matrix.argtypes = [ctypes.c_int, ctypes.c_int, P]
+    L.pll_dct2d_exact.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, P, P]
+    rng = np.random.default_rng(5)
+    N, n = 300, 41
+    a = rng.uniform(-1, -0.1, (N, n)); c = rng.uniform(-1, -0.1, (N, n))
+    b = 3 + rng.uniform(0, 1, (N, n)); r = rng.standard_normal((N, n))
+    gb, gc, gr = tridiag_batch(a, b, c, r)
+    for s in range(N):
+        bb, cc, rr = b[s].copy(), c[s].copy(), r[s].copy()
+        L.orc_thomas_pll(n, a[s].ctypes.data_as(P), bb.ctypes.data_as(P),
+                         cc.ctypes.data_as(P), rr.ctypes.data_as(P))
+        assert np.array_equal(gr[s], rr) and np.array_equal(gb[s], bb) and np.array_equal(gc[s], cc)
+    n0, n1, hm = 12, 20, 5
+    x = rng.standard_normal((hm, n0, n1))
+    for kind in (0, 1):
+        T0 = np.zeros((n0, n0)); T1 = np.zeros((n1, n1))
+        L.pll_dct_matrix(kind, n0, T0.ctypes.data_as(P)); L.pll_dct_matrix(kind, n1, T1.ctypes.data_as(P))
+        g = dct2d_batch(kind, x)
+        for t in range(hm):
+            out = np.zeros((n0, n1)); tmp = np.zeros((n0, n1)); xi = np.ascontiguousarray(x[t])
+            L.pll_dct2d_exact(kind, n0, n1, T0.ctypes.data_as(P), T1.ctypes.data_as(P),
+                              xi.ctypes.data_as(P), out.ctypes.data_as(P), tmp.ctypes.data_as(P))
+            assert np.array_equal(g[t], out)
