@@ -211,7 +211,7 @@ def run_ours(args, ws, rank, local):
     prm = wl.params
     cells = prm.cells
     ic = workload_fields(wl)
-    s = Solver(prm, device=local, exact_dct=True, use_graph=True)
+    s = Solver(prm, device=local, exact_dct=False, use_graph=True)
     s.load_ic(ic)
     stream = torch.cuda.ExternalStream(s._L.pllgpu_stream(s._h), device=local)
 

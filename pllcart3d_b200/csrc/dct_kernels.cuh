@@ -82,4 +82,81 @@ __global__ void __launch_bounds__(256) k_gemm_seq(GemmDesc d, const real* __rest
     }
 }
 
+
+// Same contraction on the FP64 tensor cores: mma.sync m8n8k4 .f64 (DMMA),
+// FP64 products and FP64 accumulation in the tensor pipe (the order of the
+// k-sum differs from the sequential loop, so results agree with k_gemm_seq
+// to rounding).  64x64 block tile, 8 warps as 2 (m) x 4 (n), each warp a
+// 32x16 sub-tile of 4x2 m8n8 fragments; k tiles of 16 through shared memory.
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(256) k_gemm_dmma(GemmDesc d, const double* __restrict__ A,
+                                                   const double* __restrict__ B, double* __restrict__ C)
+{
+    constexpr int TM = 64, TN = 64, TK = 16, PAD = 4;
+    __shared__ double As[TK][TM + PAD];
+    __shared__ double Bs[TK][TN + PAD];
+    const int b = blockIdx.z;
+    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wm = warp >> 2, wn = warp & 3;   // 2 x 4 warps
+    const int g = lane >> 2, tg = lane & 3;    // fragment group / thread in group
+    const double* Ab = A + (long)b * d.sAb;
+    const double* Bb = B + (long)b * d.sBb;
+    double acc[4][2][2];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) acc[p][q][0] = acc[p][q][1] = 0.0;
+    for (int k0 = 0; k0 < d.K; k0 += TK) {
+        for (int t = threadIdx.x; t < TK * TM; t += 256) {
+            const int kk = d.sAk == 1 ? t % TK : t / TM, mm = d.sAk == 1 ? t / TK : t % TM;
+            const int m = m0 + mm, k = k0 + kk;
+            As[kk][mm] = (m < d.M && k < d.K) ? Ab[(long)m * d.sAm + (long)k * d.sAk] : 0.0;
+        }
+        for (int t = threadIdx.x; t < TK * TN; t += 256) {
+            const int kk = d.sBk == 1 ? t % TK : t / TN, nn = d.sBk == 1 ? t / TK : t % TN;
+            const int n = n0 + nn, k = k0 + kk;
+            Bs[kk][nn] = (n < d.N && k < d.K) ? Bb[(long)k * d.sBk + (long)n * d.sBn] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < TK; kk += 4) {
+            double a[4], bv[2];
+#pragma unroll
+            for (int p = 0; p < 4; ++p) a[p] = As[kk + tg][wm * 32 + p * 8 + g];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) bv[q] = Bs[kk + tg][wn * 16 + q * 8 + g];
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+#pragma unroll
+                for (int q = 0; q < 2; ++q) dmma_8x8x4(acc[p][q][0], acc[p][q][1], a[p], bv[q]);
+        }
+        __syncthreads();
+    }
+    double* Cb = C + (long)b * d.sCb;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const int m = m0 + wm * 32 + p * 8 + g;
+        if (m >= d.M) continue;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int n = n0 + wn * 16 + q * 8 + 2 * tg + h;
+                if (n >= d.N) continue;
+                double v = acc[p][q][h];
+                if (d.scale_mode == 1) v = v * d.scale;
+                else if (d.scale_mode == 2) v = v / d.scale;
+                Cb[(long)m * d.sCm + (long)n * d.sCn] = v;
+            }
+        }
+    }
+}
+
 }  // namespace pll

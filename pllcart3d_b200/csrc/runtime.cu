@@ -92,6 +92,8 @@ struct pllgpu_ctx {
     int* status = nullptr;      // device sticky status bits
     double* work = nullptr;     // slope-parameter scratch
     int cur = 0;                // buffer index holding the "old" role
+    bool rotated = false;       // fast steps ran: "new" roles are stale and
+                                // logically equal to "old" (see materialize)
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     bool graphs_ready = false;
     double timestep = 0;
@@ -202,8 +204,11 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
     k_adi_yz<VAR, 1, double><<<dim3((nk(R) + 127) / 128, ni(R)), 128, 0, ctx->st>>>(
         ctx->G, R, ctx->K, mn, ctx->S, ctx->cc, ctx->scal, alpha);
     mark(ctx, VAR == VC ? "adi_y_c" : VAR == VU ? "adi_y_u" : VAR == VV ? "adi_y_v" : "adi_y_w");
-    k_adi_yz<VAR, 2, double><<<dim3((nj(R) + 127) / 128, ni(R)), 128, 0, ctx->st>>>(
-        ctx->G, R, ctx->K, mn, ctx->S, ctx->cc, ctx->scal, alpha);
+    {
+        constexpr size_t smem = adi_z_smem_bytes<VAR, double>();
+        k_adi_z_tiled<VAR, double><<<dim3((nj(R) + 127) / 128, ni(R)), 128, smem, ctx->st>>>(
+            ctx->G, R, ctx->K, mn, ctx->S, ctx->cc, ctx->scal, alpha);
+    }
     mark(ctx, VAR == VC ? "adi_z_c" : VAR == VU ? "adi_z_u" : VAR == VV ? "adi_z_v" : "adi_z_w");
     XsweepArgs<double> X;
     X.mu = mn;
@@ -233,7 +238,10 @@ void launch_viscosity(pllgpu_ctx* ctx, const double* cn, MuPtrs<double> m)
 void launch_gemm(pllgpu_ctx* ctx, const GemmDesc& d, const double* A, const double* B, double* C)
 {
     dim3 grid((d.N + 63) / 64, (d.M + 63) / 64, d.batch);
-    k_gemm_seq<double><<<grid, 256, 0, ctx->st>>>(d, A, B, C);
+    if (ctx->P.exact_dct)
+        k_gemm_seq<double><<<grid, 256, 0, ctx->st>>>(d, A, B, C);
+    else
+        k_gemm_dmma<<<grid, 256, 0, ctx->st>>>(d, A, B, C);
     mark(ctx, "dct_gemm");
 }
 
@@ -532,6 +540,15 @@ pllgpu_ctx* pllgpu_create(const pllgpu_params* p, int device)
         pllgpu_destroy(ctx);
         return nullptr;
     }
+    // kernels above the 48 KB default of dynamic shared memory
+    cudaFuncSetAttribute(k_adi_z_tiled<VC, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)adi_z_smem_bytes<VC, double>());
+    cudaFuncSetAttribute(k_adi_z_tiled<VU, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)adi_z_smem_bytes<VU, double>());
+    cudaFuncSetAttribute(k_adi_z_tiled<VV, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)adi_z_smem_bytes<VV, double>());
+    cudaFuncSetAttribute(k_adi_z_tiled<VW, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)adi_z_smem_bytes<VW, double>());
     // DCT matrices and Poisson eigenvalues (phisolver_dct L2050-2051)
     {
         const double PI = 4.0 * std::atan(1.0);
@@ -596,7 +613,59 @@ int pllgpu_field_id(const char* name)
     return -1;
 }
 
-static double* field_ptr(pllgpu_ctx* ctx, int f)
+// After fast steps the reference's state has new == old (update_old_*
+// copies); the ping-pong buffers hold a stale "new".  Reads of new-role
+// fields then see the old-role buffer; writes first copy old -> new.
+static bool is_new_role(int f)
+{
+    return f == PLLGPU_C_NEW || f == PLLGPU_C_HN || f == PLLGPU_U_NEW || f == PLLGPU_U_HN ||
+           f == PLLGPU_V_NEW || f == PLLGPU_V_HN || f == PLLGPU_W_NEW || f == PLLGPU_W_HN ||
+           (f >= PLLGPU_MU_NEW_CELL && f <= PLLGPU_MU_NEW_YZ);
+}
+
+static int new_to_old(int f)
+{
+    switch (f) {
+    case PLLGPU_C_NEW: return PLLGPU_C_OLD;
+    case PLLGPU_C_HN: return PLLGPU_C_HNM1;
+    case PLLGPU_U_NEW: return PLLGPU_U_OLD;
+    case PLLGPU_U_HN: return PLLGPU_U_HNM1;
+    case PLLGPU_V_NEW: return PLLGPU_V_OLD;
+    case PLLGPU_V_HN: return PLLGPU_V_HNM1;
+    case PLLGPU_W_NEW: return PLLGPU_W_OLD;
+    case PLLGPU_W_HN: return PLLGPU_W_HNM1;
+    default: return f - (PLLGPU_MU_NEW_CELL - PLLGPU_MU_OLD_CELL);
+    }
+}
+
+static int materialize(pllgpu_ctx* ctx)
+{
+    if (!ctx->rotated) return PLLGPU_OK;
+    const size_t bytes = sizeof(double) * (size_t)ctx->nelem;
+    for (int v = 0; v < 4; ++v) {
+        CK(cudaMemcpyAsync(ctx->q_new(v), ctx->q_old(v), bytes, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->h_n(v), ctx->h_nm1(v), bytes, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->mu[1 - ctx->cur][v], ctx->mu[ctx->cur][v], bytes, cudaMemcpyDeviceToDevice,
+                           ctx->st));
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->rotated = false;
+    return PLLGPU_OK;
+}
+
+static double* field_ptr_raw(pllgpu_ctx* ctx, int f);
+
+static double* field_ptr(pllgpu_ctx* ctx, int f, bool for_write)
+{
+    if (f < 0 || f >= PLLGPU_NFIELDS) return nullptr;
+    if (ctx->rotated && is_new_role(f)) {
+        if (!for_write) return field_ptr_raw(ctx, new_to_old(f));
+        if (materialize(ctx)) return nullptr;
+    }
+    return field_ptr_raw(ctx, f);
+}
+
+static double* field_ptr_raw(pllgpu_ctx* ctx, int f)
 {
     if (f < 0 || f >= PLLGPU_NFIELDS) return nullptr;
     if (f <= PLLGPU_C_HNM1) {
@@ -625,7 +694,7 @@ int pllgpu_dims(const pllgpu_ctx* ctx, int* d)
 int pllgpu_set_field(pllgpu_ctx* ctx, int f, const double* host)
 {
     if (!ctx || !host) return PLLGPU_EINVAL;
-    double* d = field_ptr(ctx, f);
+    double* d = field_ptr(ctx, f, true);
     if (!d) return fail(ctx, PLLGPU_EINVAL);
     const Geo& G = ctx->G;
     CK(cudaMemcpy2DAsync(d, sizeof(double) * G.sy, host, sizeof(double) * G.NZ, sizeof(double) * G.NZ,
@@ -637,7 +706,7 @@ int pllgpu_set_field(pllgpu_ctx* ctx, int f, const double* host)
 int pllgpu_get_field(pllgpu_ctx* ctx, int f, double* host)
 {
     if (!ctx || !host) return PLLGPU_EINVAL;
-    double* d = field_ptr(ctx, f);
+    double* d = field_ptr(ctx, f, false);
     if (!d) return fail(ctx, PLLGPU_EINVAL);
     const Geo& G = ctx->G;
     CK(cudaMemcpy2DAsync(host, sizeof(double) * G.NZ, d, sizeof(double) * G.sy, sizeof(double) * G.NZ,
@@ -649,7 +718,7 @@ int pllgpu_get_field(pllgpu_ctx* ctx, int f, double* host)
 int pllgpu_device_field(pllgpu_ctx* ctx, int f, double** dptr, long* si, long* sj)
 {
     if (!ctx) return PLLGPU_EINVAL;
-    double* d = field_ptr(ctx, f);
+    double* d = field_ptr(ctx, f, true);
     if (!d) return PLLGPU_EINVAL;
     if (dptr) *dptr = d;
     if (si) *si = ctx->G.sx;
@@ -661,6 +730,7 @@ int pllgpu_start(pllgpu_ctx* ctx)
 {
     if (!ctx) return PLLGPU_EINVAL;
     CK(cudaSetDevice(ctx->dev));
+    if (int e = materialize(ctx)) return e;
     const size_t bytes = sizeof(double) * (size_t)ctx->nelem;
     // update_ghost_points (L81) on the initial velocities; phi is zero
     launch_project(ctx, 0.0, 0, 1, 0);
@@ -705,6 +775,7 @@ int pllgpu_steps(pllgpu_ctx* ctx, int nsteps)
             if (int e = check_launch(ctx)) return e;
         }
     }
+    if (nsteps > 0) ctx->rotated = true;
     CK(cudaStreamSynchronize(ctx->st));
     return read_status(ctx);
 }
@@ -729,6 +800,8 @@ int pllgpu_routine(pllgpu_ctx* ctx, int routine, const double* in, double* out)
 {
     if (!ctx || routine < 0 || routine >= PLLGPU_NROUTINES) return PLLGPU_EINVAL;
     CK(cudaSetDevice(ctx->dev));
+    if (routine != PLLGPU_R_SUBSTEP)
+        if (int e = materialize(ctx)) return e;
     double dt = in ? in[0] : 0.0, g = in ? in[1] : 0.0, r = in ? in[2] : 0.0, vb = in ? in[3] : 0.0;
     const double alpha = g + r;
     const size_t bytes = sizeof(double) * (size_t)ctx->nelem;
@@ -801,6 +874,7 @@ int pllgpu_routine(pllgpu_ctx* ctx, int routine, const double* in, double* out)
         if (rk < 0 || rk > 2) return fail(ctx, PLLGPU_EINVAL);
         if (set_scalar(ctx, S_DT, dt)) return ctx->err;
         enqueue_substep(ctx, rk);
+        ctx->rotated = true;
         break;
     }
     default:
@@ -830,6 +904,7 @@ int pllgpu_profile_steps(pllgpu_ctx* ctx, int nsteps, int maxk, char* names, dou
         mark(ctx, "tval");
     }
     ctx->profiling = false;
+    ctx->rotated = true;
     if (int e = check_launch(ctx)) return e;
     CK(cudaStreamSynchronize(ctx->st));
     int nk = 0;

@@ -530,4 +530,138 @@ __global__ void __launch_bounds__(128) k_adi_x(Geo G, Rng R, Consts K, XsweepArg
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// ADI line solve along z (the contiguous axis), same arithmetic as
+// k_adi_yz<VAR,2>, but each warp owns 32 neighbouring lines (fixed i,
+// consecutive j) and moves them through shared memory in 32x32 tiles, so
+// that every global access is a coalesced 256-byte row segment instead of 32
+// lines' worth of strided ones.  Forward elimination writes c' to `cc` and
+// the eliminated rhs over S, tile by tile; back substitution walks the tiles
+// in reverse.
+// ---------------------------------------------------------------------------
+template <int VAR, typename real>
+constexpr size_t adi_z_smem_bytes()
+{
+    return sizeof(real) * 4 * 32 * (2 * 33 + (VAR == VC ? 0 : 34));
+}
+
+template <int VAR, typename real>
+__global__ void __launch_bounds__(128) k_adi_z_tiled(Geo G, Rng R, Consts K, MuPtrs<real> mu,
+                                                     real* __restrict__ S, real* __restrict__ cc,
+                                                     const double* __restrict__ scal, double alpha)
+{
+    constexpr int W = 32;
+    // dynamic shared memory: per warp an S tile, a c' tile and (momentum) a
+    // viscosity tile; adi_z_smem_bytes() gives the size
+    extern __shared__ __align__(16) unsigned char zsm[];
+    typedef real Tile[W][W + 1];
+    typedef real MTile[W][W + 2];
+    Tile* tS = (Tile*)zsm;
+    Tile* tC = tS + 4;
+    MTile* tM = (MTile*)(tC + 4);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = R.is + blockIdx.y;
+    const int j0 = R.js + (blockIdx.x * 4 + warp) * W;
+    if (j0 > R.je) return;  // warp-uniform
+    const int nl = (R.je - j0 + 1) < W ? (R.je - j0 + 1) : W;
+    const int n = R.ke - R.ks + 1;
+    const real fac = (real)(0.5 * scal[S_DT] * alpha);
+    constexpr int LO = Closure<VAR, 2>::lo, HI = Closure<VAR, 2>::hi;
+    const real* __restrict__ mz = VAR == VU ? mu.xz : VAR == VV ? mu.yz : mu.cell;
+    const int moff = VAR == VW ? -1 : 0;
+    const double dz_coef = VAR == VW ? K.d2z : K.d1z;
+    const long base0 = (long)i * G.sx + (long)j0 * G.sy + R.ks;
+    real cprev = 0, rprev = 0;
+    for (int k0 = 0; k0 < n; k0 += W) {
+        const int nk = (n - k0) < W ? (n - k0) : W;
+        for (int r = 0; r < nl; ++r) {
+            const long b = base0 + (long)r * G.sy + k0;
+            if (lane < nk) tS[warp][r][lane] = S[b + lane];
+            if (VAR != VC) {
+                if (lane < nk) tM[warp][r][lane] = mz[b + moff + lane];
+                if (lane == 0) tM[warp][r][nk] = mz[b + moff + nk];
+            }
+        }
+        __syncwarp();
+        if (lane < nl) {
+            for (int t = 0; t < nk; ++t) {
+                const int m = k0 + t;
+                real a, c;
+                if (VAR == VC) {
+                    a = (real)K.cdz;
+                    c = (real)K.cdz;
+                } else {
+                    a = over_h<real>((real)dz_coef * tM[warp][lane][t], K.hz, K.ihz, K.pow2);
+                    c = over_h<real>((real)dz_coef * tM[warp][lane][t + 1], K.hz, K.ihz, K.pow2);
+                }
+                const real b = -(a + c);
+                real la = -fac * a, lb = (real)1.0 - fac * b, lc = -fac * c, lr = tS[warp][lane][t];
+                if (m == 0) {
+                    if (LO == 1) lb += la;
+                    else if (LO == 2) lb -= la;
+                    else if (LO == 3) lr -= la * (real)0.0;
+                }
+                if (m == n - 1) {
+                    if (HI == 1) lb += lc;
+                    else if (HI == 2) lb -= lc;
+                    else if (HI == 3) lr -= lc * (real)0.0;
+                }
+                real bb, cm, rm;
+                if (m == 0) {
+                    bb = lb;
+                    cm = lc / bb;
+                    rm = lr / bb;
+                } else {
+                    bb = lb - cprev * la;
+                    cm = lc / bb;
+                    rm = (lr - rprev * la) / bb;
+                }
+                tC[warp][lane][t] = cm;
+                tS[warp][lane][t] = rm;
+                cprev = cm;
+                rprev = rm;
+            }
+        }
+        __syncwarp();
+        for (int r = 0; r < nl; ++r) {
+            const long b = base0 + (long)r * G.sy + k0;
+            if (lane < nk) {
+                S[b + lane] = tS[warp][r][lane];
+                cc[b + lane] = tC[warp][r][lane];
+            }
+        }
+        __syncwarp();
+    }
+    // back substitution, last tile first; x_{n-1} = r'_{n-1}
+    real xnext = rprev;
+    const int last0 = ((n - 1) / W) * W;
+    for (int k0 = last0; k0 >= 0; k0 -= W) {
+        const int nk = (n - k0) < W ? (n - k0) : W;
+        for (int r = 0; r < nl; ++r) {
+            const long b = base0 + (long)r * G.sy + k0;
+            if (lane < nk) {
+                tS[warp][r][lane] = S[b + lane];
+                tC[warp][r][lane] = cc[b + lane];
+            }
+        }
+        __syncwarp();
+        if (lane < nl) {
+            for (int t = nk - 1; t >= 0; --t) {
+                const int m = k0 + t;
+                if (m == n - 1) continue;
+                real x = tS[warp][lane][t] - xnext * tC[warp][lane][t];
+                tS[warp][lane][t] = x;
+                xnext = x;
+            }
+        }
+        __syncwarp();
+        for (int r = 0; r < nl; ++r) {
+            const long b = base0 + (long)r * G.sy + k0;
+            if (lane < nk) S[b + lane] = tS[warp][r][lane];
+        }
+        __syncwarp();
+    }
+}
+
 }  // namespace pll

@@ -27,7 +27,7 @@ def _dp(a: np.ndarray):
 
 
 class Solver:
-    def __init__(self, params: Params, device: int = 0, exact_dct: bool = True,
+    def __init__(self, params: Params, device: int = 0, exact_dct: bool = False,
                  use_graph: bool = True):
         params.validate()
         self.params = params

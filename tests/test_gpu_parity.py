@@ -12,7 +12,7 @@ import pytest
 from oracle.pyref import FIELDS, OracleRun
 from pllcart3d_b200.ic import workload_fields
 from pllcart3d_b200.params import workload
-from tests.util import STATE_FIELDS, rel_maxnorm
+from tests.util import STATE_FIELDS, rel_maxnorm, rel_vector
 
 pytestmark = pytest.mark.gpu
 
@@ -25,23 +25,25 @@ def _solver(params, **kw):
     return Solver(params, **kw)
 
 
-def _pair(name, warm_steps=1, **kw):
+def _pair(name, warm_steps=1, exact_dct=False, **kw):
     wl = workload(name)
     wl.params = wl.params.replace(**kw)
     ic = workload_fields(wl)
     o = OracleRun(wl.params, ic)
     o.steps(warm_steps)
-    s = _solver(wl.params)
+    s = _solver(wl.params, exact_dct=exact_dct)
     s.load_ic(ic)
     for f in FIELDS:
         s.set(f, o.get(f))
     return wl, o, s
 
 
-def _cmp(s, o, names, tol=TOL):
+def _cmp(s, o, names, tol=TOL, vector=True):
+    """relative max-norm per field; with vector=True velocity-like
+    components are scaled by their vector's max-norm"""
     worst = {}
     for f in names:
-        e = rel_maxnorm(s.get(f), o.get(f))
+        e = rel_vector(s.get, o.get, f) if vector else rel_maxnorm(s.get(f), o.get(f))
         worst[f] = e
         assert e <= tol, f"{f}: rel err {e:.3e} > {tol}"
     return worst
@@ -83,7 +85,7 @@ def test_routines_one_by_one(name, kw):
 
 def test_routines_without_exp_are_bitwise():
     """Stages that do not call exp() reproduce the restatement exactly."""
-    wl, o, s = _pair("fingering-16x8x8", warm_steps=3)
+    wl, o, s = _pair("fingering-16x8x8", warm_steps=3, exact_dct=True)
     dt, g, r = o.step_dt(), 8.0 / 15.0, 0.0
     vb = o.bulk_velo()
     o.call("concentration", dt, g, r, vb); s.concentration(dt, g, r, vb)
@@ -94,12 +96,14 @@ def test_routines_without_exp_are_bitwise():
     assert np.array_equal(s.get("phi"), o.get("phi"))
 
 
-@pytest.mark.parametrize("name,steps,kw", [
-    ("fingering-64x32x32", 200, {}),
-    ("fingering-20x6x9", 30, {"Fx": 1.0, "Fy": 2.0}),
-    ("fingering-18x9x7", 20, {"Nmvp": 1, "Vratio": 1.0}),
+@pytest.mark.parametrize("name,steps,kw,per_field", [
+    # the 64x32x32 case of the headline parity target: every field on its
+    # own max-norm, c, u, v, w, phi and the pressure gradients
+    ("fingering-64x32x32", 200, {}, True),
+    ("fingering-20x6x9", 30, {"Fx": 1.0, "Fy": 2.0}, False),
+    ("fingering-18x9x7", 20, {"Nmvp": 1, "Vratio": 1.0}, False),
 ])
-def test_full_steps_match_oracle(name, steps, kw):
+def test_full_steps_match_oracle(name, steps, kw, per_field):
     wl = workload(name)
     wl.params = wl.params.replace(**kw)
     ic = workload_fields(wl)
@@ -109,7 +113,10 @@ def test_full_steps_match_oracle(name, steps, kw):
     s.step(steps)
     o.steps(steps)
     assert s.dt == pytest.approx(o.dt, rel=1e-12)
-    _cmp(s, o, STATE_FIELDS)
+    # after whole steps the reference's new arrays equal the old ones
+    for q in "cuvw":
+        assert np.array_equal(s.get(f"{q}_new"), s.get(f"{q}_old"))
+    _cmp(s, o, STATE_FIELDS, vector=not per_field)
 
 
 def test_graph_and_stream_paths_agree():
