@@ -201,15 +201,6 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
     const Rng& R = ctx->Rv[VAR];
     const double alpha = g + r;
     MuPtrs<double> mn = ctx->mu_new();
-    k_adi_yz<VAR, 1, double><<<dim3((nk(R) + 127) / 128, ni(R)), 128, 0, ctx->st>>>(
-        ctx->G, R, ctx->K, mn, ctx->S, ctx->cc, ctx->scal, alpha);
-    mark(ctx, VAR == VC ? "adi_y_c" : VAR == VU ? "adi_y_u" : VAR == VV ? "adi_y_v" : "adi_y_w");
-    {
-        constexpr size_t smem = adi_z_smem_bytes<VAR, double>();
-        k_adi_z_tiled<VAR, double><<<dim3((nj(R) + 127) / 128, ni(R)), 128, smem, ctx->st>>>(
-            ctx->G, R, ctx->K, mn, ctx->S, ctx->cc, ctx->scal, alpha);
-    }
-    mark(ctx, VAR == VC ? "adi_z_c" : VAR == VU ? "adi_z_u" : VAR == VV ? "adi_z_v" : "adi_z_w");
     XsweepArgs<double> X;
     X.mu = mn;
     X.q = ctx->q_old(VAR);
@@ -222,7 +213,15 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
     X.g = g;
     X.r = r;
     X.alpha = alpha;
-    k_adi_x<VAR, double><<<dim3((nk(R) + 127) / 128, nj(R)), 128, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
+    k_line_pf<VAR, 1, double><<<dim3((nk(R) + 63) / 64, ni(R)), 64, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
+    mark(ctx, VAR == VC ? "adi_y_c" : VAR == VU ? "adi_y_u" : VAR == VV ? "adi_y_v" : "adi_y_w");
+    {
+        constexpr size_t smem = adi_z_smem_bytes<VAR, double>();
+        k_adi_z_tiled<VAR, double><<<dim3((nj(R) + 127) / 128, ni(R)), 128, smem, ctx->st>>>(
+            ctx->G, R, ctx->K, mn, ctx->S, ctx->cc, ctx->scal, alpha);
+    }
+    mark(ctx, VAR == VC ? "adi_z_c" : VAR == VU ? "adi_z_u" : VAR == VV ? "adi_z_v" : "adi_z_w");
+    k_line_pf<VAR, 0, double><<<dim3((nk(R) + 63) / 64, nj(R)), 64, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
     mark(ctx, VAR == VC ? "adi_x_c" : VAR == VU ? "adi_x_u" : VAR == VV ? "adi_x_v" : "adi_x_w");
 }
 

@@ -36,6 +36,8 @@ struct Consts {
     double M, Vnorm;
 };
 
+enum { MU_CELL_ = 0, MU_XY_ = 1, MU_XZ_ = 2, MU_YZ_ = 3 };
+
 template <typename real>
 __device__ __forceinline__ real over_h(real x, double h, double ih, int pow2)
 {
@@ -661,6 +663,232 @@ __global__ void __launch_bounds__(128) k_adi_z_tiled(Geo G, Rng R, Consts K, MuP
             if (lane < nk) S[b + lane] = tS[warp][r][lane];
         }
         __syncwarp();
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// Viscosity family and offset that the implicit coefficients of VAR along
+// AXIS read (A_umom/A_vmom/A_wmom, pllcart3d.c:1443-1536): a at line
+// position m uses family[m + OFF], c uses family[m + OFF + 1]; the scale is
+// 2/(Re h) on the variable's own axis and 1/(Re h) across.
+// ---------------------------------------------------------------------------
+template <int VAR, int AXIS>
+struct LineCoef {
+    static constexpr int fam = VAR == VC ? -1
+                             : (VAR == VU && AXIS == 0) || (VAR == VV && AXIS == 1) || (VAR == VW && AXIS == 2) ? MU_CELL_
+                             : (VAR == VU && AXIS == 1) || (VAR == VV && AXIS == 0) ? MU_XY_
+                             : (VAR == VU && AXIS == 2) || (VAR == VW && AXIS == 0) ? MU_XZ_
+                                                                                      : MU_YZ_;
+    static constexpr int off = fam == MU_CELL_ ? -1 : 0;
+    static constexpr bool twice = fam == MU_CELL_;
+};
+
+template <int VAR, int AXIS, typename real>
+__device__ __forceinline__ const real* line_family(const MuPtrs<real>& mu)
+{
+    constexpr int f = LineCoef<VAR, AXIS>::fam;
+    return f == MU_CELL_ ? mu.cell : f == MU_XY_ ? mu.xy : f == MU_XZ_ ? mu.xz : mu.yz;
+}
+
+// a, c of the ADI operator from two consecutive family values (same
+// expressions as acoef)
+template <int VAR, int AXIS, typename real>
+__device__ __forceinline__ void line_ac(const Consts& K, real m0, real m1, real& a, real& c)
+{
+    const double h = AXIS == 0 ? K.hx : AXIS == 1 ? K.hy : K.hz;
+    const double ih = AXIS == 0 ? K.ihx : AXIS == 1 ? K.ihy : K.ihz;
+    if (VAR == VC) {
+        a = c = (real)(AXIS == 0 ? K.cdx : AXIS == 1 ? K.cdy : K.cdz);
+    } else {
+        const double d = LineCoef<VAR, AXIS>::twice ? (AXIS == 0 ? K.d2x : AXIS == 1 ? K.d2y : K.d2z)
+                                                     : (AXIS == 0 ? K.d1x : AXIS == 1 ? K.d1y : K.d1z);
+        a = over_h<real>((real)d * m0, h, ih, K.pow2);
+        c = over_h<real>((real)d * m1, h, ih, K.pow2);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Line solves along a strided axis (AXIS 0: x, lines (j,k); AXIS 1: y,
+// lines (i,k)), one thread per line, adjacent threads on adjacent k so every
+// access is coalesced.  The loads of PF line positions ahead (rhs and one
+// viscosity value per position) are issued before the dependent Thomas
+// recurrence consumes them, so the sweep streams instead of waiting one
+// memory latency per position.  AXIS 1 is tridiag_1rhs (pllcart3d.c:3511);
+// AXIS 0 is pll_tridiag's one-rank form with the convective outflow, the
+// q_new update and (for c) the Neumann ghosts, as k_adi_x.
+// ---------------------------------------------------------------------------
+template <int VAR, int AXIS, typename real>
+__global__ void __launch_bounds__(128) k_line_pf(Geo G, Rng R, Consts K, XsweepArgs<real> A)
+{
+    constexpr int PF = 8;
+    const int k = R.ks + blockIdx.x * blockDim.x + threadIdx.x;
+    const int o = blockIdx.y;  // j (AXIS 0) or i (AXIS 1) offset
+    if (k > R.ke) return;
+    const long st = AXIS == 0 ? G.sx : G.sy;
+    const int n = AXIS == 0 ? R.ie - R.is + 1 : R.je - R.js + 1;
+    const long base = AXIS == 0 ? (long)R.is * G.sx + (long)(R.js + o) * G.sy + k
+                                : (long)(R.is + o) * G.sx + (long)R.js * G.sy + k;
+    const real dt = (real)A.scal[S_DT];
+    const real fac = (real)(0.5 * A.scal[S_DT] * A.alpha);
+    constexpr int LO = Closure<VAR, AXIS>::lo, HI = Closure<VAR, AXIS>::hi;
+    constexpr int OFF = LineCoef<VAR, AXIS>::off;
+    const real* __restrict__ fam = VAR == VC ? nullptr : line_family<VAR, AXIS, real>(A.mu);
+    real* __restrict__ S = A.S;
+    real* __restrict__ cc = A.cc;
+
+    real boun = 0;
+    if (AXIS == 0) {
+        const long rb = base + (long)n * st;
+        real Hb = -(real)A.scal[S_VBULK] * (A.q[rb] - A.q[rb - st]);
+        Hb = over_h<real>(Hb, K.hx, K.ihx, K.pow2);
+        A.H[rb] = Hb;
+        boun = dt * ((real)A.g * Hb + (real)A.r * A.Hm[rb]);
+        A.qn[rb] = A.q[rb] + boun;
+    }
+
+    // forward elimination
+    real cprev = 0, rprev = 0;
+    real mlast = VAR == VC ? (real)0 : fam[base + (long)OFF * st];
+    real sv[PF], mv[PF];
+#pragma unroll
+    for (int t = 0; t < PF; ++t) {
+        sv[t] = t < n ? S[base + (long)t * st] : (real)0;
+        if (VAR != VC) mv[t] = t < n ? fam[base + (long)(t + OFF + 1) * st] : (real)0;
+    }
+    for (int m0 = 0; m0 < n; m0 += PF) {
+        real sn[PF], mn[PF];
+#pragma unroll
+        for (int t = 0; t < PF; ++t) {
+            const int m = m0 + PF + t;
+            sn[t] = m < n ? S[base + (long)m * st] : (real)0;
+            if (VAR != VC) mn[t] = m < n ? fam[base + (long)(m + OFF + 1) * st] : (real)0;
+        }
+#pragma unroll
+        for (int t = 0; t < PF; ++t) {
+            const int m = m0 + t;
+            if (m < n) {
+                real a, c;
+                line_ac<VAR, AXIS, real>(K, mlast, VAR == VC ? (real)0 : mv[t], a, c);
+                if (VAR != VC) mlast = mv[t];
+                const real b = -(a + c);
+                real la = -fac * a, lb = (real)1.0 - fac * b, lc = -fac * c, lr = sv[t];
+                if (m == 0) {
+                    if (LO == 1) lb += la;
+                    else if (LO == 2) lb -= la;
+                    else if (LO == 3) lr -= la * (real)0.0;
+                }
+                if (m == n - 1) {
+                    if (AXIS == 0) lr -= lc * boun;
+                    else if (HI == 1) lb += lc;
+                    else if (HI == 2) lb -= lc;
+                    else if (HI == 3) lr -= lc * (real)0.0;
+                }
+                real cm, rm;
+                if (AXIS == 0) {
+                    if (m == 0) {
+                        lb = lb - (real)0.0 * la;
+                        cm = lc / lb;
+                        rm = (lr - (real)0.0 * la) / lb;
+                    } else {
+                        lb = (lb - cprev * la);
+                        cm = lc / lb;
+                        rm = (lr - rprev * la) / lb;
+                    }
+                } else {
+                    if (m == 0) {
+                        cm = lc / lb;
+                        rm = lr / lb;
+                    } else {
+                        const real bb = lb - cprev * la;
+                        cm = lc / bb;
+                        rm = (lr - rprev * la) / bb;
+                    }
+                }
+                const long id = base + (long)m * st;
+                cc[id] = cm;
+                S[id] = rm;
+                cprev = cm;
+                rprev = rm;
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < PF; ++t) {
+            sv[t] = sn[t];
+            if (VAR != VC) mv[t] = mn[t];
+        }
+    }
+
+    // back substitution, x_{n-1} = r'_{n-1} (pll form: minus c' * 0)
+    real xnext = AXIS == 0 ? rprev - cprev * (real)0.0 : rprev;
+    if (AXIS == 0) {
+        const long id = base + (long)(n - 1) * st;
+        A.qn[id] = A.q[id] + xnext;
+    }
+    // positions n-2 .. 0 in chunks of PF, loads of the next chunk first
+    real rv[PF], cv[PF], qv[PF];
+    int mtop = n - 2;
+#pragma unroll
+    for (int t = 0; t < PF; ++t) {
+        const int m = mtop - t;
+        const long id = base + (long)m * st;
+        rv[t] = m >= 0 ? S[id] : (real)0;
+        cv[t] = m >= 0 ? cc[id] : (real)0;
+        if (AXIS == 0) qv[t] = m >= 0 ? A.q[id] : (real)0;
+    }
+    for (; mtop >= 0; mtop -= PF) {
+        real rn[PF], cn2[PF], qn2[PF];
+#pragma unroll
+        for (int t = 0; t < PF; ++t) {
+            const int m = mtop - PF - t;
+            const long id = base + (long)m * st;
+            rn[t] = m >= 0 ? S[id] : (real)0;
+            cn2[t] = m >= 0 ? cc[id] : (real)0;
+            if (AXIS == 0) qn2[t] = m >= 0 ? A.q[id] : (real)0;
+        }
+#pragma unroll
+        for (int t = 0; t < PF; ++t) {
+            const int m = mtop - t;
+            if (m >= 0) {
+                const long id = base + (long)m * st;
+                real x = AXIS == 0 ? rv[t] - cv[t] * xnext : rv[t] - xnext * cv[t];
+                if (AXIS == 0) A.qn[id] = qv[t] + x;
+                else S[id] = x;
+                xnext = x;
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < PF; ++t) {
+            rv[t] = rn[t];
+            cv[t] = cn2[t];
+            if (AXIS == 0) qv[t] = qn2[t];
+        }
+    }
+
+    if (AXIS == 0 && VAR == VC) {
+        // Neumann ghosts of c (pllcart3d.c:700-712), as in k_adi_x
+        const long sy = G.sy;
+        const int j = R.js + o;
+        const bool jlo = (j == R.js), jhi = (j == R.je);
+        const bool klo = (k == R.ks), khi = (k == R.ke);
+        if (jlo | jhi | klo | khi) {
+            for (int m = 0; m < n; ++m) {
+                const long id = base + (long)m * st;
+                const real v = A.qn[id];
+                if (jlo) A.qn[id - sy] = v;
+                if (jhi) A.qn[id + sy] = v;
+                if (klo) {
+                    A.qn[id - 1] = v;
+                    if (jlo) A.qn[id - sy - 1] = v;
+                    if (jhi) A.qn[id + sy - 1] = v;
+                }
+                if (khi) {
+                    A.qn[id + 1] = v;
+                    if (jlo) A.qn[id - sy + 1] = v;
+                    if (jhi) A.qn[id + sy + 1] = v;
+                }
+            }
+        }
     }
 }
 
