@@ -92,6 +92,10 @@ enum {
     PLLGPU_R_BULK_VELO,           /* bulk_velo L3381-3398 -> out[0]           */
     PLLGPU_R_FIND_CFL,            /* find_cfl L3095-3118 -> out[0]            */
     PLLGPU_R_SUBSTEP,             /* one RK substep L164-194: dt, rk          */
+    PLLGPU_R_VISCOSITY_EXP,       /* calculate_viscosity(c_new) L843-886,
+                                     mu = exp(M c) whatever Nmvp is           */
+    PLLGPU_R_VISCOSITY_NMVP,      /* calculate_viscosity_nmvp L889-948: cm    */
+    PLLGPU_R_SLOPE_PARAMETER,     /* slope_parameter(c_new) L722-840 -> out[0]*/
     PLLGPU_NROUTINES
 };
 
@@ -133,6 +137,28 @@ void *pllgpu_stream(pllgpu_ctx *ctx);
  * device time in ms and the number of launches; *nk = labels filled */
 int pllgpu_profile_steps(pllgpu_ctx *ctx, int nsteps, int maxk, char *names,
                          double *total_ms, int *launches, int *nk);
+
+/* Timestep after the diffusive cap (pllcart3d.c:150-154) and the simulated
+ * time, for hosts that run their own start-up */
+int pllgpu_set_timestep(pllgpu_ctx *ctx, double timestep);
+int pllgpu_set_tval(pllgpu_ctx *ctx, double tval);
+/* implicit-operator coefficients of variable var (0 c, 1 u, 2 v, 3 w) from
+ * the mu_old (which=0) or mu_new (which=1) arrays, A_conc/A_umom/A_vmom/
+ * A_wmom (pllcart3d.c:1411-1536): abc9 holds 9 padded fields (a,b,c of x,
+ * then y, then z), filled on the variable's unknown range, 0 elsewhere */
+int pllgpu_acoef(pllgpu_ctx *ctx, int var, int which, double *abc9);
+
+/* calculate_weno (pllcart3d.c:3455-3507) for n points: v5 holds the five
+ * divided differences d1[kk + sign*m], m = 0..4, of each point */
+int pllgpu_weno_batch(int n, const double *v5, double *out);
+/* tridiag_1rhs (pllcart3d.c:3511-3536) for N systems of length n, host
+ * buffers as pllgpu_tridiag_batch; a, b, c are left untouched */
+int pllgpu_tridiag_1rhs_batch(int N, int n, const double *a, const double *b,
+                              const double *c, double *r);
+/* idct_3d's transform (fftw_3d.h:77-106): REDFT01 in both dimensions
+ * followed by the division by 4*n0*n1 */
+int pllgpu_idct2d_batch(int n0, int n1, int howmany, const double *in,
+                        double *out);
 
 /*
  * Batched line solve of pll_tridiag (pll_tridiag.c:152-158) on one rank:

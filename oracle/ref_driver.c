@@ -86,12 +86,14 @@ static Conc *g_c;
 static Visc *g_mu_old, *g_mu_new;
 static double ***g_phi, ***g_div;
 static double g_tval, g_dt, g_cm;
+static char g_rundir[4096]; /* where the reference's side files go */
 
 int pllref_init(const char *rundir)
 {
     char here[4096];
     if (!getcwd(here, sizeof(here))) return -1;
     if (chdir(rundir) != 0) return -1;
+    strncpy(g_rundir, rundir, sizeof(g_rundir) - 1);
     Rank = 0;
     Size = 1;
     input();
@@ -217,6 +219,9 @@ int pllref_load_ic(const double *c, const double *u, const double *v,
                    const double *w)
 {
     double del_min, diff_dt;
+    char here[4096];
+    /* slope_parameter appends to Outscreen in the working directory */
+    if (!getcwd(here, sizeof(here)) || chdir(g_rundir) != 0) return -1;
     pllref_set("c_new", c);
     pllref_set("u_new", u);
     pllref_set("v_new", v);
@@ -239,6 +244,7 @@ int pllref_load_ic(const double *c, const double *u, const double *v,
     diff_dt = 0.1 * Pe * del_min * del_min;
     Timestep = (diff_dt < Timestep) ? diff_dt : Timestep;
     g_tval = 0.0;
+    if (chdir(here) != 0) return -1;
     return 0;
 }
 
@@ -364,3 +370,85 @@ double pllref_calculate_weno(double *d1, int kk, int sign)
 {
     return calculate_weno(d1, kk, sign);
 }
+
+/* The time-step loop of pllcart3d.c:158-195 with any of its routines taken
+ * from a table of replacements (NULL entries keep the reference's own):
+ * 0 concentration 1 calculate_viscosity 2 xmom 3 ymom 4 zmom
+ * 5 update_velo_boundary 6 divergence 7 phisolver_dct 8 update_phi_ghosts
+ * 9 velo_correction 10 update_veloghost_points 11 pressure_gradient
+ * 12 update_old_conc 13 update_old_velo 14 update_old_visc 15 find_cfl
+ * 16 bulk_velo.  Used to run the drop-in layer inside the reference's own
+ * loop, on the reference's own structures. */
+typedef void (*conc_fn)(double, double, double, double, Grid *, double ***, double ***, double ***, Conc *);
+typedef void (*visc_fn)(Grid *, double ***, Visc *);
+typedef void (*mom_fn)(double, double, double, double, Grid *, Visc *, Visc *, double ***, double ***,
+                       double ***, Velo *);
+typedef void (*zmom_fn)(double, double, double, double, Grid *, Visc *, Visc *, double ***, double ***, Velo *);
+typedef void (*vb_fn)(Grid *, Velo *, Velo *, Velo *);
+typedef void (*div_fn)(Grid *, double ***, double ***, double ***, double ***);
+typedef void (*phi_fn)(double, double, double, Grid *, double ***, double ***);
+typedef void (*phig_fn)(Grid *, double ***);
+typedef void (*corr_fn)(double, double, double, Grid *, double ***, Velo *, Velo *, Velo *);
+typedef void (*oc_fn)(Conc *);
+typedef void (*ov_fn)(Velo *, Velo *, Velo *);
+typedef void (*om_fn)(Visc *, Visc *);
+typedef double (*cfl_fn)(Grid *, double ***, double ***, double ***);
+typedef double (*bulk_fn)(Grid *, double ***);
+
+int pllref_steps_with(int n, void **f)
+{
+    int s, rk;
+#define PICK(i, T, dflt) ((f && f[i]) ? (T)f[i] : (T)dflt)
+    conc_fn f_conc = PICK(0, conc_fn, concentration);
+    visc_fn f_visc = PICK(1, visc_fn, calculate_viscosity);
+    mom_fn f_x = PICK(2, mom_fn, xmom), f_y = PICK(3, mom_fn, ymom);
+    zmom_fn f_z = PICK(4, zmom_fn, zmom);
+    vb_fn f_vb = PICK(5, vb_fn, update_velo_boundary);
+    div_fn f_div = PICK(6, div_fn, divergence);
+    phi_fn f_phi = PICK(7, phi_fn, phisolver_dct);
+    phig_fn f_phig = PICK(8, phig_fn, update_phi_ghosts);
+    corr_fn f_corr = PICK(9, corr_fn, velo_correction);
+    vb_fn f_vg = PICK(10, vb_fn, update_veloghost_points);
+    corr_fn f_pg = PICK(11, corr_fn, pressure_gradient);
+    oc_fn f_oc = PICK(12, oc_fn, update_old_conc);
+    ov_fn f_ov = PICK(13, ov_fn, update_old_velo);
+    om_fn f_om = PICK(14, om_fn, update_old_visc);
+    cfl_fn f_cfl = PICK(15, cfl_fn, find_cfl);
+    bulk_fn f_bulk = PICK(16, bulk_fn, bulk_velo);
+#undef PICK
+    for (s = 0; s < n; s++) {
+        double cfl_dt = f_cfl(g_grid, g_u->old, g_v->old, g_w->old);
+        g_dt = (cfl_dt < Timestep) ? cfl_dt : Timestep;
+        for (rk = 0; rk < 3; rk++) {
+            double g = RK1[rk], r = RK2[rk], vbulk;
+            g_tval = g_tval + (g + r) * g_dt;
+            vbulk = f_bulk(g_grid, g_u->old);
+            f_conc(g_dt, g, r, vbulk, g_grid, g_u->new, g_v->new, g_w->new, g_c);
+            f_visc(g_grid, g_c->new, g_mu_new);
+            f_x(g_dt, g, r, vbulk, g_grid, g_mu_old, g_mu_new, g_c->new, g_v->old, g_w->old, g_u);
+            f_y(g_dt, g, r, vbulk, g_grid, g_mu_old, g_mu_new, g_c->new, g_u->old, g_w->old, g_v);
+            f_z(g_dt, g, r, vbulk, g_grid, g_mu_old, g_mu_new, g_u->old, g_v->old, g_w);
+            f_vb(g_grid, g_u, g_v, g_w);
+            f_div(g_grid, g_u->new, g_v->new, g_w->new, g_div);
+            f_phi(g_dt, g, r, g_grid, g_div, g_phi);
+            f_phig(g_grid, g_phi);
+            f_corr(g_dt, g, r, g_grid, g_phi, g_u, g_v, g_w);
+            f_vg(g_grid, g_u, g_v, g_w);
+            f_pg(g_dt, g, r, g_grid, g_phi, g_u, g_v, g_w);
+            f_oc(g_c);
+            f_ov(g_u, g_v, g_w);
+            f_om(g_mu_old, g_mu_new);
+        }
+    }
+    return 0;
+}
+
+/* the reference's own structures, for hosts that hand them to another
+ * implementation (the resident GPU path) */
+void pllref_structs(void **out)
+{
+    out[0] = g_grid; out[1] = g_u; out[2] = g_v; out[3] = g_w; out[4] = g_c;
+    out[5] = g_mu_old; out[6] = g_mu_new; out[7] = g_phi;
+}
+
+void pllref_set_tval(double t) { g_tval = t; }

@@ -34,7 +34,8 @@ ROUTINES = {
     "concentration": 0, "viscosity_new": 1, "xmom": 2, "ymom": 3, "zmom": 4,
     "velo_ghosts": 5, "divergence": 6, "phisolver": 7, "phi_ghosts": 8,
     "velo_correction": 9, "pressure_gradient": 10, "rotate": 11,
-    "bulk_velo": 12, "find_cfl": 13, "substep": 14,
+    "bulk_velo": 12, "find_cfl": 13, "substep": 14, "viscosity_exp": 15,
+    "viscosity_nmvp": 16, "slope_parameter": 17,
 }
 
 ERRORS = {0: "ok", 1: "NaN or Inf in the velocity field", 2: "CUDA error",
@@ -102,6 +103,12 @@ def lib():
                                        ctypes.POINTER(_I), ctypes.POINTER(_I)]
     L.pllgpu_tridiag_batch.argtypes = [_I, _I, _PD, _PD, _PD, _PD]
     L.pllgpu_dct2d_batch.argtypes = [_I, _I, _I, _I, _PD, _PD]
+    L.pllgpu_set_timestep.argtypes = [_VP, _D]
+    L.pllgpu_set_tval.argtypes = [_VP, _D]
+    L.pllgpu_acoef.argtypes = [_VP, _I, _I, _PD]
+    L.pllgpu_weno_batch.argtypes = [_I, _PD, _PD]
+    L.pllgpu_tridiag_1rhs_batch.argtypes = [_I, _I, _PD, _PD, _PD, _PD]
+    L.pllgpu_idct2d_batch.argtypes = [_I, _I, _I, _PD, _PD]
     _lib = L
     return L
 
@@ -114,4 +121,6 @@ EXPORTED_SYMBOLS = [
     "pllgpu_timestep", "pllgpu_tval", "pllgpu_error_string",
     "pllgpu_kernels_per_step", "pllgpu_tridiag_batch", "pllgpu_dct2d_batch",
     "pllgpu_stream", "pllgpu_profile_steps",
+    "pllgpu_set_timestep", "pllgpu_set_tval", "pllgpu_acoef", "pllgpu_weno_batch",
+    "pllgpu_tridiag_1rhs_batch", "pllgpu_idct2d_batch",
 ]

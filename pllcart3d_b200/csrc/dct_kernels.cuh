@@ -95,7 +95,7 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
                  : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(256) k_gemm_dmma(GemmDesc d, const double* __restrict__ A,
+static __global__ void __launch_bounds__(256) k_gemm_dmma(GemmDesc d, const double* __restrict__ A,
                                                    const double* __restrict__ B, double* __restrict__ C)
 {
     constexpr int TM = 64, TN = 64, TK = 16, PAD = 4;

@@ -225,11 +225,11 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
     mark(ctx, VAR == VC ? "adi_x_c" : VAR == VU ? "adi_x_u" : VAR == VV ? "adi_x_v" : "adi_x_w");
 }
 
-void launch_viscosity(pllgpu_ctx* ctx, const double* cn, MuPtrs<double> m)
+void launch_viscosity(pllgpu_ctx* ctx, const double* cn, MuPtrs<double> m, int law = -1)
 {
     dim3 blk(32, 4);
     k_viscosity<double><<<box_grid(ctx->G.NZ, ctx->G.NY, ni(ctx->Rg) + 2, blk), blk, 0, ctx->st>>>(
-        ctx->G, ctx->Rg, ctx->K, ctx->P.nmvp, cn, (double*)m.cell, (double*)m.xy, (double*)m.xz,
+        ctx->G, ctx->Rg, ctx->K, law < 0 ? ctx->P.nmvp : law, cn, (double*)m.cell, (double*)m.xy, (double*)m.xz,
         (double*)m.yz, ctx->scal);
     mark(ctx, "viscosity");
 }
@@ -868,6 +868,31 @@ int pllgpu_routine(pllgpu_ctx* ctx, int routine, const double* in, double* out)
         launch_cfl(ctx);
         if (out) out[0] = get_scalar(ctx, S_CFLDT);
         break;
+    case PLLGPU_R_VISCOSITY_EXP:
+        launch_viscosity(ctx, ctx->q_new(VC), ctx->mu_new(), 0);
+        break;
+    case PLLGPU_R_VISCOSITY_NMVP: {
+        // coefficients of calculate_viscosity_nmvp (pllcart3d.c:895-900)
+        const double cm = dt, PI = 4.0 * std::atan(1.0), M = ctx->P.Vratio;
+        const double alpha = std::exp(M), mum = ctx->P.Mum * alpha;
+        const double psi0 = std::asin(alpha / mum), psi1 = PI - std::asin(1 / mum);
+        const double etam = (PI / 2 - psi0) / (psi1 - psi0);
+        const double a = ((1 - cm) - etam) / ((1 - cm) * (etam - 1));
+        if (set_scalar(ctx, S_CM, cm) || set_scalar(ctx, S_MUM, mum) || set_scalar(ctx, S_PSI0, psi0) ||
+            set_scalar(ctx, S_PSI1, psi1) || set_scalar(ctx, S_NMVA, a))
+            return ctx->err;
+        launch_viscosity(ctx, ctx->q_new(VC), ctx->mu_new(), 1);
+        break;
+    }
+    case PLLGPU_R_SLOPE_PARAMETER: {
+        const double PI = 4.0 * std::atan(1.0);
+        k_slope_parameter<<<1, 1, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->P.Y1, ctx->P.Z1, ctx->G.dy, ctx->G.dz,
+                                                ctx->P.Vratio, ctx->P.Mum, ctx->P.Lambda, PI, ctx->q_new(VC),
+                                                ctx->scal, ctx->status, ctx->work);
+        mark(ctx, "slope_parameter");
+        if (out) out[0] = get_scalar(ctx, S_CM);
+        break;
+    }
     case PLLGPU_R_SUBSTEP: {
         const int rk = (int)g;
         if (rk < 0 || rk > 2) return fail(ctx, PLLGPU_EINVAL);
@@ -1033,6 +1058,164 @@ extern "C" int pllgpu_dct2d_batch(int kind, int n0, int n1, int howmany, const d
     // along the slow dimension: y[t][k][c] = sum_r T0[k][r] tmp[t][r][c]
     GemmDesc d2{n0, n1, n0, howmany, 0, n0, 1, per, n1, 1, per, n1, 1, 0.0, 0};
     k_gemm_seq<double><<<dim3((n1 + 63) / 64, (n0 + 63) / 64, howmany), 256>>>(d2, dT0.d(), dtmp.d(), dy.d());
+    if (cudaGetLastError() != cudaSuccess) return PLLGPU_ECUDA;
+    if (cudaMemcpy(out, dy.p, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return PLLGPU_ECUDA;
+    return PLLGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// coefficient export, setters and stand-alone primitives of the drop-in layer
+// ---------------------------------------------------------------------------
+namespace {
+
+template <int VAR>
+__global__ void k_acoef(Geo G, Rng R, Consts K, MuPtrs<double> mu, double* __restrict__ abc, long nelem)
+{
+    const int k = R.ks + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = R.js + blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = R.is + blockIdx.z;
+    if (k > R.ke || j > R.je) return;
+    const long id = (long)i * G.sx + (long)j * G.sy + k;
+    double a, b, c;
+    acoef<VAR, 0, double>(K, G, mu.cell, mu.xy, mu.xz, mu.yz, id, a, b, c);
+    abc[id] = a; abc[nelem + id] = b; abc[2 * nelem + id] = c;
+    acoef<VAR, 1, double>(K, G, mu.cell, mu.xy, mu.xz, mu.yz, id, a, b, c);
+    abc[3 * nelem + id] = a; abc[4 * nelem + id] = b; abc[5 * nelem + id] = c;
+    acoef<VAR, 2, double>(K, G, mu.cell, mu.xy, mu.xz, mu.yz, id, a, b, c);
+    abc[6 * nelem + id] = a; abc[7 * nelem + id] = b; abc[8 * nelem + id] = c;
+}
+
+__global__ void k_weno_batch(int n, const double* __restrict__ v5, double* __restrict__ out)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const double* v = v5 + 5L * t;
+    out[t] = weno5<double>(v[0], v[1], v[2], v[3], v[4]);
+}
+
+// tridiag_1rhs on N contiguous systems; c' in scratch cc
+__global__ void k_tridiag_1rhs_batch(int N, int n, const double* __restrict__ a, const double* __restrict__ b,
+                                     const double* __restrict__ c, double* __restrict__ r, double* __restrict__ cc)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= N) return;
+    const long o = (long)s * n;
+    double bb = b[o];
+    cc[o] = c[o] / bb;
+    r[o] = r[o] / bb;
+    for (int i = 1; i < n; ++i) {
+        bb = b[o + i] - cc[o + i - 1] * a[o + i];
+        cc[o + i] = c[o + i] / bb;
+        r[o + i] = (r[o + i] - r[o + i - 1] * a[o + i]) / bb;
+    }
+    for (int i = n - 2; i >= 0; --i) r[o + i] = r[o + i] - r[o + i + 1] * cc[o + i];
+}
+
+__global__ void k_divide(long n, double* __restrict__ x, double d)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) x[t] = x[t] / d;
+}
+
+}  // namespace
+
+extern "C" int pllgpu_set_timestep(pllgpu_ctx* ctx, double ts)
+{
+    if (!ctx) return PLLGPU_EINVAL;
+    ctx->timestep = ts;
+    return set_scalar(ctx, S_TIMESTEP, ts);
+}
+
+extern "C" int pllgpu_set_tval(pllgpu_ctx* ctx, double t)
+{
+    if (!ctx) return PLLGPU_EINVAL;
+    return set_scalar(ctx, S_TVAL, t);
+}
+
+extern "C" int pllgpu_acoef(pllgpu_ctx* ctx, int var, int which, double* abc9)
+{
+    if (!ctx || var < 0 || var > 3 || (which != 0 && which != 1) || !abc9) return PLLGPU_EINVAL;
+    CK(cudaSetDevice(ctx->dev));
+    if (int e = materialize(ctx)) return e;
+    const long ne = ctx->nelem;
+    DevBuf buf;
+    if (!buf.alloc(sizeof(double) * 9 * (size_t)ne)) return fail(ctx, PLLGPU_ECUDA);
+    CK(cudaMemsetAsync(buf.p, 0, sizeof(double) * 9 * (size_t)ne, ctx->st));
+    MuPtrs<double> m = which ? ctx->mu_new() : ctx->mu_old();
+    const Rng& R = ctx->Rv[var];
+    dim3 blk(32, 4), grd = box_grid(nk(R), nj(R), ni(R), blk);
+    if (var == VC) k_acoef<VC><<<grd, blk, 0, ctx->st>>>(ctx->G, R, ctx->K, m, buf.d(), ne);
+    else if (var == VU) k_acoef<VU><<<grd, blk, 0, ctx->st>>>(ctx->G, R, ctx->K, m, buf.d(), ne);
+    else if (var == VV) k_acoef<VV><<<grd, blk, 0, ctx->st>>>(ctx->G, R, ctx->K, m, buf.d(), ne);
+    else k_acoef<VW><<<grd, blk, 0, ctx->st>>>(ctx->G, R, ctx->K, m, buf.d(), ne);
+    if (int e = check_launch(ctx)) return e;
+    const Geo& G = ctx->G;
+    for (int f = 0; f < 9; ++f)
+        CK(cudaMemcpy2DAsync(abc9 + (long)f * G.NX * G.NY * G.NZ, sizeof(double) * G.NZ, buf.d() + (long)f * ne,
+                             sizeof(double) * G.sy, sizeof(double) * G.NZ, (size_t)G.NX * G.NY,
+                             cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return PLLGPU_OK;
+}
+
+extern "C" int pllgpu_weno_batch(int n, const double* v5, double* out)
+{
+    if (n < 0 || !v5 || !out) return PLLGPU_EINVAL;
+    if (n == 0) return PLLGPU_OK;
+    DevBuf dv, dout;
+    if (!dv.alloc(sizeof(double) * 5 * (size_t)n) || !dout.alloc(sizeof(double) * (size_t)n)) return PLLGPU_ECUDA;
+    if (cudaMemcpy(dv.p, v5, sizeof(double) * 5 * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess)
+        return PLLGPU_ECUDA;
+    k_weno_batch<<<(n + 127) / 128, 128>>>(n, dv.d(), dout.d());
+    if (cudaGetLastError() != cudaSuccess) return PLLGPU_ECUDA;
+    if (cudaMemcpy(out, dout.p, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return PLLGPU_ECUDA;
+    return PLLGPU_OK;
+}
+
+extern "C" int pllgpu_tridiag_1rhs_batch(int N, int n, const double* a, const double* b, const double* c,
+                                         double* r)
+{
+    if (N < 0 || n < 1 || !a || !b || !c || !r) return PLLGPU_EINVAL;
+    if (N == 0) return PLLGPU_OK;
+    const size_t bytes = sizeof(double) * (size_t)N * n;
+    DevBuf da, db, dc, dr, dcc;
+    if (!da.alloc(bytes) || !db.alloc(bytes) || !dc.alloc(bytes) || !dr.alloc(bytes) || !dcc.alloc(bytes))
+        return PLLGPU_ECUDA;
+    if (cudaMemcpy(da.p, a, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(db.p, b, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dc.p, c, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dr.p, r, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        return PLLGPU_ECUDA;
+    k_tridiag_1rhs_batch<<<(N + 127) / 128, 128>>>(N, n, da.d(), db.d(), dc.d(), dr.d(), dcc.d());
+    if (cudaGetLastError() != cudaSuccess) return PLLGPU_ECUDA;
+    if (cudaMemcpy(r, dr.p, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return PLLGPU_ECUDA;
+    return PLLGPU_OK;
+}
+
+extern "C" int pllgpu_idct2d_batch(int n0, int n1, int howmany, const double* in, double* out)
+{
+    if (n0 < 1 || n1 < 1 || howmany < 0 || !in || !out) return PLLGPU_EINVAL;
+    if (howmany == 0) return PLLGPU_OK;
+    const long per = (long)n0 * n1, tot = per * howmany;
+    const size_t bytes = sizeof(double) * (size_t)tot;
+    std::vector<double> T0((size_t)n0 * n0), T1((size_t)n1 * n1);
+    dct_matrix(1, n0, T0.data());
+    dct_matrix(1, n1, T1.data());
+    DevBuf dT0, dT1, dx, dtmp, dy;
+    if (!dT0.alloc(sizeof(double) * T0.size()) || !dT1.alloc(sizeof(double) * T1.size()) || !dx.alloc(bytes) ||
+        !dtmp.alloc(bytes) || !dy.alloc(bytes))
+        return PLLGPU_ECUDA;
+    if (cudaMemcpy(dT0.p, T0.data(), sizeof(double) * T0.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dT1.p, T1.data(), sizeof(double) * T1.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dx.p, in, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        return PLLGPU_ECUDA;
+    GemmDesc d1{n0, n1, n1, howmany, per, n1, 1, 0, 1, n1, per, n1, 1, 0.0, 0};
+    k_gemm_seq<double><<<dim3((n1 + 63) / 64, (n0 + 63) / 64, howmany), 256>>>(d1, dx.d(), dT1.d(), dtmp.d());
+    GemmDesc d2{n0, n1, n0, howmany, 0, n0, 1, per, n1, 1, per, n1, 1, 0.0, 0};
+    k_gemm_seq<double><<<dim3((n1 + 63) / 64, (n0 + 63) / 64, howmany), 256>>>(d2, dT0.d(), dtmp.d(), dy.d());
+    // fftw_3d.h:101 divides by (double)(4*N)
+    k_divide<<<(int)((tot + 255) / 256), 256>>>(tot, dy.d(), (double)(4 * per));
     if (cudaGetLastError() != cudaSuccess) return PLLGPU_ECUDA;
     if (cudaMemcpy(out, dy.p, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return PLLGPU_ECUDA;
     return PLLGPU_OK;
