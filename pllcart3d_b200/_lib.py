@@ -109,6 +109,7 @@ def lib():
     L.pllgpu_weno_batch.argtypes = [_I, _PD, _PD]
     L.pllgpu_tridiag_1rhs_batch.argtypes = [_I, _I, _PD, _PD, _PD, _PD]
     L.pllgpu_idct2d_batch.argtypes = [_I, _I, _I, _PD, _PD]
+    L.pllgpu_dct2d_batch_noalloc.argtypes = [_I, _I, _I, _I, _VP, _VP, _VP]
     _lib = L
     return L
 
@@ -120,7 +121,7 @@ EXPORTED_SYMBOLS = [
     "pllgpu_sync", "pllgpu_status", "pllgpu_clear_status", "pllgpu_last_dt",
     "pllgpu_timestep", "pllgpu_tval", "pllgpu_error_string",
     "pllgpu_kernels_per_step", "pllgpu_tridiag_batch", "pllgpu_dct2d_batch",
-    "pllgpu_stream", "pllgpu_profile_steps",
+    "pllgpu_stream", "pllgpu_profile_steps", "pllgpu_dct2d_batch_noalloc",
     "pllgpu_set_timestep", "pllgpu_set_tval", "pllgpu_acoef", "pllgpu_weno_batch",
     "pllgpu_tridiag_1rhs_batch", "pllgpu_idct2d_batch",
 ]

@@ -27,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--fmad=false",
               "-Xcompiler", "-fPIC", "-Xptxas", "-warn-spills"]
 
-CU_SOURCES = ["runtime.cu"]
+CU_SOURCES = ["runtime.cu", "noalloc.cu"]
 HEADERS = ["common.cuh", "step_kernels.cuh", "aux_kernels.cuh", "dct_kernels.cuh"]
 
 
