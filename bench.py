@@ -6,7 +6,10 @@
 
 One step = one full RK3-CN time step (pllcart3d.c:158-195) of the named
 seeded synthetic fingering workload (default fingering-512x256x256, the size
-the headline metric is quoted at).  The FP64 state arrays are each 282 MB,
+the headline metric is quoted at).  Both precision forms are timed: the
+headline `value` is the precision form (FP32 state, split-TF32 DCT, FP64
+Poisson mode solve), the plain FP64 form is reported beside it
+(`fp64_form`, `mixed_over_fp64`).  Every state array is at least 141 MB,
 larger than the 126 MB L2, so no L2 flush is needed between steps.
 
 --impl ours       the GPU step through the pllgpu_ C ABI (one CUDA graph per
@@ -49,6 +52,9 @@ def parse():
     ap.add_argument("--workload", default="fingering-512x256x256")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
+                    help="forms to time; the headline value is --headline's")
+    ap.add_argument("--headline", default="mixed", choices=["fp64", "mixed"])
     return ap.parse_args()
 
 
@@ -199,23 +205,18 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args, ws, rank, local):
-    import numpy as np
+def measure(prm, ic, form, steps, warmup, ws, local, profile_steps=2):
+    """Device-timed steps of one precision form + per-kernel event profile."""
+    import ctypes
+
     import torch
 
-    from pllcart3d_b200 import _lib
     from pllcart3d_b200.solver import Solver
 
-    torch.cuda.set_device(local)
-    wl = workload(args.workload)
-    prm = wl.params
-    cells = prm.cells
-    ic = workload_fields(wl)
-    s = Solver(prm, device=local, exact_dct=False, use_graph=True)
+    s = Solver(prm, device=local, exact_dct=False, use_graph=True, precision=form)
     s.load_ic(ic)
     stream = torch.cuda.ExternalStream(s._L.pllgpu_stream(s._h), device=local)
-
-    s.step(args.warmup)
+    s.step(warmup)
     barrier(ws)
     clocks = Clocks(local)
     clocks.start()
@@ -223,48 +224,75 @@ def run_ours(args, ws, rank, local):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    s.step(args.steps)
+    s.step(steps)
     e1.record(stream)
     torch.cuda.synchronize()
     barrier(ws)
     ms = e0.elapsed_time(e1)
     ck = clocks.stop()
     ms_max = reduce_max(ms, ws)
-    value = cells * args.steps * ws / (ms_max / 1e3)
-    launches = s.kernels_per_step * args.steps
-
-    # per-kernel device times of the same step (stream launches + events)
-    import ctypes
-
     maxk = 64
     names = ctypes.create_string_buffer(32 * maxk)
     tot = (ctypes.c_double * maxk)()
     cnt = (ctypes.c_int * maxk)()
     nk = ctypes.c_int(0)
-    nprof = 2
-    code = s._L.pllgpu_profile_steps(s._h, nprof, maxk, names, tot, cnt, ctypes.byref(nk))
     kernels = {}
-    if code == 0:
+    if s._L.pllgpu_profile_steps(s._h, profile_steps, maxk, names, tot, cnt, ctypes.byref(nk)) == 0:
         for t in range(nk.value):
             lab = names.raw[32 * t:32 * t + 32].split(b"\0")[0].decode()
             kernels[lab] = {"ms_total": tot[t], "launches": cnt[t]}
-    step_ms_prof = sum(v["ms_total"] for v in kernels.values()) / nprof
+    out = {"ms": ms_max, "launches_per_step": s.kernels_per_step, "clocks": ck,
+           "kernels": kernels, "profile_steps": profile_steps, "solver": s}
+    return out
+
+
+def roofline_of(kernels, nprof, cells, precision):
     hbm, peak_kind = peaks()
-    roof = None
     cand = {k: v for k, v in kernels.items() if k in roofline.KERNEL_WORDS}
-    if cand:
-        top = max(cand, key=lambda k: cand[k]["ms_total"])
-        avg_ms = cand[top]["ms_total"] / cand[top]["launches"]
-        alg = roofline.kernel_bytes_per_launch(top, cells)
-        ach = alg / (avg_ms / 1e3) / 1e9
-        roof = {"kernel": top, "bound": "hbm", "achieved": ach, "peak": hbm,
-                "unit": "GB/s", "frac": ach / hbm, "traffic": None,
-                "peak_source": peak_kind,
-                "share_of_step": cand[top]["ms_total"] / nprof / step_ms_prof}
-    step_bytes = roofline.step_bytes(cells)
-    step_roof = {"bytes_per_step": step_bytes,
-                 "achieved_gbs": step_bytes / (ms / args.steps / 1e3) / 1e9,
-                 "frac_of_hbm": step_bytes / (ms / args.steps / 1e3) / 1e9 / hbm}
+    if not cand:
+        return None
+    step_ms_prof = sum(v["ms_total"] for v in kernels.values()) / nprof
+    top = max(cand, key=lambda k: cand[k]["ms_total"])
+    avg_ms = cand[top]["ms_total"] / cand[top]["launches"]
+    alg = roofline.kernel_bytes_per_launch(top, cells, precision)
+    ach = alg / (avg_ms / 1e3) / 1e9
+    return {"kernel": top, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+            "frac": ach / hbm, "traffic": None, "peak_source": peak_kind,
+            "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
+            "share_of_step": cand[top]["ms_total"] / nprof / step_ms_prof}
+
+
+def run_ours(args, ws, rank, local):
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from pllcart3d_b200 import _lib
+
+    torch.cuda.set_device(local)
+    wl = workload(args.workload)
+    prm = wl.params
+    cells = prm.cells
+    ic = workload_fields(wl)
+    hbm, _ = peaks()
+
+    forms = {}
+    for form in (("fp64", "mixed") if args.precision == "both" else (args.precision,)):
+        m = measure(prm, ic, form, args.steps, args.warmup, ws, local)
+        prec = "fp32" if form == "mixed" else "fp64"
+        sb = roofline.step_bytes(cells, prec)
+        m["value"] = cells * args.steps * ws / (m["ms"] / 1e3)
+        m["roofline"] = roofline_of(m["kernels"], m["profile_steps"], cells, prec)
+        m["step_roofline"] = {"bytes_per_step": sb,
+                              "achieved_gbs": sb / (m["ms"] / args.steps / 1e3) / 1e9,
+                              "frac_of_hbm": sb / (m["ms"] / args.steps / 1e3) / 1e9 / hbm}
+        forms[form] = m
+        if form != args.headline:
+            m["solver"].close()
+
+    head = forms[args.headline]
+    s = head["solver"]
 
     e2e = None
     if not args.no_e2e:
@@ -273,9 +301,8 @@ def run_ours(args, ws, rank, local):
         for t, k in zip(pin[:4], "cuvw"):
             t.numpy()[...] = ic[k]
         ptr = [ctypes.cast(t.data_ptr(), ctypes.POINTER(ctypes.c_double)) for t in pin]
-        s2 = s
         t0 = time.perf_counter()
-        code = s2._L.pllgpu_run_host(s2._h, args.steps, *ptr)
+        code = s._L.pllgpu_run_host(s._h, args.steps, *ptr)
         t1 = time.perf_counter()
         if code != 0:
             raise _lib.PllGpuError(code, "run_host")
@@ -284,9 +311,10 @@ def run_ours(args, ws, rank, local):
         e2e = {"value": cells * args.steps * ws / sec, "unit": "cell-steps/s",
                "h2d_bytes_per_step": nbytes / args.steps,
                "d2h_bytes_per_step": nbytes / args.steps,
-               "note": "pllgpu_run_host: initial c,u,v,w from pinned host memory, "
-                       f"{args.steps} steps, c,u,v,w back to pinned host memory, "
+               "note": "pllgpu_run_host: initial c,u,v,w (FP64) from pinned host memory, "
+                       f"start-up, {args.steps} steps, c,u,v,w back to pinned host memory, "
                        "wall-clock around the call"}
+    s.close()
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -300,19 +328,27 @@ def run_ours(args, ws, rank, local):
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": ws,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "metric": METRIC, "value": head["value"], "unit": "cell-steps/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
+            "dtype": "f32" if args.headline == "mixed" else "f64", "data": "synthetic",
             "config": {"workload": wl.name, "grid": [prm.nx, prm.ny, prm.nz],
-                       "precision": "fp64", "parallelism": "replicas" if ws > 1 else "single",
-                       "l2": "inputs larger than L2 (282 MB per field)"},
-            "e2e": e2e, "gpu_launches": launches, "roofline": roof,
-            "step_roofline": step_roof, "cpu_baseline": cpu, "clocks": ck,
-            "kernels_ms_per_step": {k: v["ms_total"] / nprof for k, v in kernels.items()},
+                       "precision": args.headline,
+                       "parallelism": "replicas" if ws > 1 else "single",
+                       "l2": "inputs larger than L2 (each field >= 141 MB)"},
+            "e2e": e2e, "gpu_launches": head["launches_per_step"] * args.steps,
+            "roofline": head["roofline"], "step_roofline": head["step_roofline"],
+            "cpu_baseline": cpu, "clocks": head["clocks"],
+            "kernels_ms_per_step": {k: v["ms_total"] / head["profile_steps"]
+                                    for k, v in head["kernels"].items()},
         }
+        for form, m in forms.items():
+            line[f"{form}_form"] = {"value": m["value"], "ms_per_step": m["ms"] / args.steps,
+                                    "step_roofline_frac": m["step_roofline"]["frac_of_hbm"],
+                                    "roofline": m["roofline"], "clocks": m["clocks"]}
+        if "fp64" in forms and "mixed" in forms:
+            line["mixed_over_fp64"] = forms["mixed"]["value"] / forms["fp64"]["value"]
         print(json.dumps(line), flush=True)
-    s.close()
 
 
 def main():

@@ -45,6 +45,9 @@ extern "C" {
 
 /* precision forms */
 #define PLLGPU_FP64 0      /* plain: the reference's FP64 arithmetic           */
+#define PLLGPU_MIXED 1     /* FP32 state, WENO/stress/ADI in FP32, split-TF32
+                              tensor-core DCT, FP64 Poisson mode solve and
+                              FP64 reductions                                  */
 
 /* run parameters: the values of param.input that the step reads
  * (input() pllcart3d.c:271-350); M = Vratio, Vnorm = 0 (L400-403) */
@@ -53,7 +56,7 @@ typedef struct pllgpu_params {
     int nmvp;              /* Nmvp: 0 mu = exp(M c), 1 non-monotonic law      */
     double X1, X2, Y1, Y2, Z1, Z2;
     double Re, Pe, Vratio, Fx, Fy, CFLmax, Timestep, Mum, Lambda;
-    int precision;         /* PLLGPU_FP64                                      */
+    int precision;         /* PLLGPU_FP64 or PLLGPU_MIXED                      */
     int exact_dct;         /* 1: DCT sums in sequential order (bitwise with
                               the CPU restatement); 0: tensor-core DMMA        */
     int use_graph;         /* 1: replay each step as one CUDA graph            */
@@ -138,6 +141,11 @@ void *pllgpu_stream(pllgpu_ctx *ctx);
 int pllgpu_profile_steps(pllgpu_ctx *ctx, int nsteps, int maxk, char *names,
                          double *total_ms, int *launches, int *nk);
 
+/* FP64 diagnostics of the current state: out4[0] mass = sum c dV,
+ * out4[1] max |div u|, out4[2] the L2 norm of div u, out4[3] the mixing
+ * length = dx * #{x-planes with 0.01 < yz-mean of c < 0.99} (the yz mean
+ * of conc_average, pllcart3d.c:3692-3704) */
+int pllgpu_diagnostics(pllgpu_ctx *ctx, double *out4);
 /* Timestep after the diffusive cap (pllcart3d.c:150-154) and the simulated
  * time, for hosts that run their own start-up */
 int pllgpu_set_timestep(pllgpu_ctx *ctx, double timestep);

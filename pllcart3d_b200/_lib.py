@@ -103,6 +103,7 @@ def lib():
                                        ctypes.POINTER(_I), ctypes.POINTER(_I)]
     L.pllgpu_tridiag_batch.argtypes = [_I, _I, _PD, _PD, _PD, _PD]
     L.pllgpu_dct2d_batch.argtypes = [_I, _I, _I, _I, _PD, _PD]
+    L.pllgpu_diagnostics.argtypes = [_VP, _PD]
     L.pllgpu_set_timestep.argtypes = [_VP, _D]
     L.pllgpu_set_tval.argtypes = [_VP, _D]
     L.pllgpu_acoef.argtypes = [_VP, _I, _I, _PD]
@@ -123,5 +124,5 @@ EXPORTED_SYMBOLS = [
     "pllgpu_kernels_per_step", "pllgpu_tridiag_batch", "pllgpu_dct2d_batch",
     "pllgpu_stream", "pllgpu_profile_steps", "pllgpu_dct2d_batch_noalloc",
     "pllgpu_set_timestep", "pllgpu_set_tval", "pllgpu_acoef", "pllgpu_weno_batch",
-    "pllgpu_tridiag_1rhs_batch", "pllgpu_idct2d_batch",
+    "pllgpu_tridiag_1rhs_batch", "pllgpu_idct2d_batch", "pllgpu_diagnostics",
 ]

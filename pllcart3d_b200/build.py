@@ -2,7 +2,8 @@
 
 * ``libpllgpu.so``          - CUDA kernels + runtime + the ``pllgpu_`` C ABI;
   the FP64 step is compiled with ``--fmad=false`` so that no multiply-add is
-  contracted (the reference's own arithmetic has none);
+  contracted (the reference's own arithmetic has none), the precision form's
+  FP32 kernels with contraction;
 * ``libpllcart3d_dropin.so`` - the reference-signature drop-in layer (plain C,
   compiled with gcc because the reference's structures name a member ``new``).
 
@@ -24,11 +25,18 @@ LIB = os.path.join(HERE, "libpllgpu.so")
 DROPIN = os.path.join(HERE, "libpllcart3d_dropin.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--fmad=false",
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xptxas", "-warn-spills"]
 
-CU_SOURCES = ["runtime.cu", "noalloc.cu"]
-HEADERS = ["common.cuh", "step_kernels.cuh", "aux_kernels.cuh", "dct_kernels.cuh"]
+# per-source contraction: the FP64 form and everything the drop-in layer and
+# the primitives run reproduce the reference's operation order, so no
+# multiply-add is contracted there; the precision form's FP32 kernels
+# (form_f32.cu) are free to contract.
+CU_SOURCES = {"runtime.cu": "--fmad=false", "form_f64.cu": "--fmad=false",
+              "form_f32.cu": "--fmad=true", "primitives.cu": "--fmad=false",
+              "noalloc.cu": "--fmad=false"}
+HEADERS = ["common.cuh", "step_kernels.cuh", "aux_kernels.cuh", "dct_kernels.cuh", "host_util.h",
+           "ctx.cuh", "host_common.cuh", "orchestrate.cuh", "forms.h"]
 
 
 def _nvcc() -> str:
@@ -46,14 +54,14 @@ def _stale(target: str, deps) -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    deps = [os.path.join(CSRC, f) for f in CU_SOURCES + HEADERS]
+    deps = [os.path.join(CSRC, f) for f in [*CU_SOURCES, *HEADERS]]
     deps.append(os.path.join(INC, "pllcart3d_gpu.h"))
     deps.append(__file__)
     if force or _stale(LIB, deps):
         objs = []
-        for src in CU_SOURCES:
+        for src, fmad in CU_SOURCES.items():
             obj = os.path.join(CSRC, src.replace(".cu", ".o"))
-            cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, "-I", INC, "-c",
+            cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, fmad, "-I", INC, "-c",
                    os.path.join(CSRC, src), "-o", obj]
             if verbose:
                 print(" ".join(cmd))

@@ -7,6 +7,9 @@
 #include "step_kernels.cuh"
 
 namespace pll {
+// internal linkage: each translation unit (and so each precision form with
+// its own contraction flags) owns its instantiations
+namespace {
 
 // nmvp coefficient slots in the device scalar array
 enum { S_MUM = 8, S_PSI0 = 9, S_PSI1 = 10, S_NMVA = 11 };
@@ -15,7 +18,10 @@ template <typename real>
 __device__ __forceinline__ real visc_law(real cavg, const Consts& K, int nmvp,
                                          const double* __restrict__ scal)
 {
-    if (!nmvp) return (real)exp((double)((real)K.M * (cavg - (real)K.Vnorm)));
+    if (!nmvp) {
+        if (sizeof(real) == 4) return (real)expf((float)((real)K.M * (cavg - (real)K.Vnorm)));
+        return (real)exp((double)((real)K.M * (cavg - (real)K.Vnorm)));
+    }
     // calculate_viscosity_nmvp, pllcart3d.c:906-909
     const double a = scal[S_NMVA], psi0 = scal[S_PSI0], psi1 = scal[S_PSI1];
     double eta = ((1 + a) * (double)cavg) / (1 + a * (double)cavg);
@@ -92,7 +98,7 @@ __global__ void __launch_bounds__(256) k_cfl(Geo G, Rng R, Consts K, const real*
 
 // dt = min(CFLmax / max, Timestep), pllcart3d.c:159-160, 3115; clears the
 // reduction slot for the next step
-__global__ void k_dt(Consts K, double* scal)
+static __global__ void k_dt(Consts K, double* scal)
 {
     double maxall = __longlong_as_double((long long)*(unsigned long long*)(scal + S_CFLMAX));
     double cfldt = K.CFLmax / maxall;
@@ -215,50 +221,54 @@ __global__ void __launch_bounds__(128) k_div_rhs(Geo G, Rng R, Consts K, const r
 // pllcart3d.c:2040-2091): a = c = 1/dx^2, b = -2/dx^2 + lam_y + lam_z,
 // Neumann at the inlet, and at the outlet Neumann except for mode (0,0),
 // whose right ghost holds phi = 0 (the pressure gauge); pll_tridiag's
-// one-rank arithmetic.  One thread per mode; lines of stride ny*nz.
-template <typename real>
+// one-rank arithmetic.  One thread per mode; lines of stride ny*nz.  The
+// mode coefficients are stored as T (the precision form keeps them in FP32)
+// but the solve, the eigenvalue division and the zero mode are FP64, with
+// c' and the eliminated rhs in FP64 scratch.
+template <typename T>
 __global__ void __launch_bounds__(128) k_poisson_x(int nx, int ny, int nz, Consts K,
                                                    const double* __restrict__ lam_y,
                                                    const double* __restrict__ lam_z,
-                                                   real* __restrict__ hat, real* __restrict__ cc)
+                                                   T* __restrict__ hat, double* __restrict__ cc,
+                                                   double* __restrict__ rr)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ny * nz) return;
     const int jy = t / nz, kz = t % nz;
     const long st = (long)ny * nz;
-    const real a = (real)K.dx2i, c = (real)K.dx2i;
-    const real bmid = (real)(-2.0 * K.dx2i + lam_y[jy] + lam_z[kz]);
+    const double a = K.dx2i, c = K.dx2i;
+    const double bmid = -2.0 * K.dx2i + lam_y[jy] + lam_z[kz];
     const bool gauge = (jy == 0) && (kz == 0);
-    real cprev = 0, rprev = 0;
+    double cprev = 0, rprev = 0;
     for (int m = 0; m < nx; ++m) {
         const long id = t + (long)m * st;
-        real lb = bmid, lr = hat[id];
+        double lb = bmid, lr = (double)hat[id];
         if (m == 0) lb += a;
         if (m == nx - 1) {
-            if (gauge) lr -= c * (real)0.0;
+            if (gauge) lr -= c * 0.0;
             else lb += c;
         }
-        real cm, rm;
+        double cm, rm;
         if (m == 0) {
-            lb = lb - (real)0.0 * a;
+            lb = lb - 0.0 * a;
             cm = c / lb;
-            rm = (lr - (real)0.0 * a) / lb;
+            rm = (lr - 0.0 * a) / lb;
         } else {
             lb = (lb - cprev * a);
             cm = c / lb;
             rm = (lr - rprev * a) / lb;
         }
         cc[id] = cm;
-        hat[id] = rm;
+        rr[id] = rm;
         cprev = cm;
         rprev = rm;
     }
-    real xnext = rprev - cprev * (real)0.0;
-    hat[t + (long)(nx - 1) * st] = xnext;
+    double xnext = rprev - cprev * 0.0;
+    hat[t + (long)(nx - 1) * st] = (T)xnext;
     for (int m = nx - 2; m >= 0; --m) {
         const long id = t + (long)m * st;
-        real x = hat[id] - cc[id] * xnext;
-        hat[id] = x;
+        double x = rr[id] - cc[id] * xnext;
+        hat[id] = (T)x;
         xnext = x;
     }
 }
@@ -412,7 +422,7 @@ __global__ void __launch_bounds__(128) k_project(Geo G, Rng Rg, Rng Ru, Rng Rv, 
 // non-monotonic viscosity law's cm from c along the x line closest to
 // y=0, z=0; also leaves the law's coefficients (L895-900) in the scalars.
 // One thread.
-__global__ void k_slope_parameter(Geo G, Rng R, double Y1, double Z1, double dy, double dz,
+static __global__ void k_slope_parameter(Geo G, Rng R, double Y1, double Z1, double dy, double dz,
                                   double M, double Mum, double Lambda, double PI,
                                   const double* __restrict__ cn, double* scal, int* status,
                                   double* work)
@@ -473,4 +483,48 @@ __global__ void k_slope_parameter(Geo G, Rng R, double Y1, double Z1, double dy,
     scal[S_NMVA] = ((1 - cm) - etam) / ((1 - cm) * (etam - 1));
 }
 
+
+// FP64 diagnostics of the state: per x-plane sums of c over the interior
+// y-z plane (the yz mean of conc_average, pllcart3d.c:3692-3704) and the
+// divergence of the new velocities, max |div| and sum div^2.  One block per
+// x-plane; the plane sums are reduced in a fixed order (deterministic).
+template <typename real>
+__global__ void __launch_bounds__(256) k_plane_diag(Geo G, Rng R, Consts K, const real* __restrict__ c,
+                                                    const real* __restrict__ u, const real* __restrict__ v,
+                                                    const real* __restrict__ w, double* __restrict__ out)
+{
+    const int i = R.is + blockIdx.x;
+    const int nj = R.je - R.js + 1, nk = R.ke - R.ks + 1;
+    double sc = 0.0, dmax = 0.0, d2 = 0.0;
+    for (int t = threadIdx.x; t < nj * nk; t += blockDim.x) {
+        const int j = R.js + t / nk, k = R.ks + t % nk;
+        const long id = (long)i * G.sx + (long)j * G.sy + k;
+        sc += (double)c[id];
+        const double dv = ((double)u[id + G.sx] - (double)u[id]) / K.hx +
+                          ((double)v[id + G.sy] - (double)v[id]) / K.hy +
+                          ((double)w[id + 1] - (double)w[id]) / K.hz;
+        dmax = fmax(dmax, fabs(dv));
+        d2 += dv * dv;
+    }
+    __shared__ double s0[256], s1[256], s2[256];
+    s0[threadIdx.x] = sc;
+    s1[threadIdx.x] = dmax;
+    s2[threadIdx.x] = d2;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            s0[threadIdx.x] += s0[threadIdx.x + h];
+            s1[threadIdx.x] = fmax(s1[threadIdx.x], s1[threadIdx.x + h]);
+            s2[threadIdx.x] += s2[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[3 * blockIdx.x + 0] = s0[0];
+        out[3 * blockIdx.x + 1] = s1[0];
+        out[3 * blockIdx.x + 2] = s2[0];
+    }
+}
+
+}  // namespace
 }  // namespace pll

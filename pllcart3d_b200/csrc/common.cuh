@@ -56,4 +56,36 @@ enum StatusBits {
     ST_BOUNDS = 4,    // a kernel's self-check found a bad index
 };
 
+// ---------------------------------------------------------------------------
+// constants shared by the stencil kernels (host-precomputed, exact as in the
+// reference: each is the same IEEE expression the reference evaluates)
+// ---------------------------------------------------------------------------
+struct Consts {
+    double hx, hy, hz;            // dx, dy, dz
+    double ihx, ihy, ihz;         // 1/dx ... (used only when pow2)
+    double i2hx, i2hy, i2hz;      // 1/(2 dx) ... (used only when pow2)
+    int pow2;                     // all spacings are exact powers of two
+    double cdx, cdy, cdz;         // 1/(Pe h^2), A_conc (pllcart3d.c:1421-1433)
+    double d1x, d1y, d1z;         // 1/(Re h)
+    double d2x, d2y, d2z;         // 2/(Re h)
+    double xuv, xuw;              // 1/(Re dy dx), 1/(Re dz dx)  (Hu_op)
+    double xvu, xvw;              // 1/(Re dx dy), 1/(Re dz dy)  (Hv_op)
+    double xwu, xwv;              // 1/(Re dx dz), 1/(Re dy dz)  (Hw_op)
+    double FxRe, FyRe;            // -(Fx/Re), -(Fy/Re)
+    double Re;
+    double area;                  // (Y2-Y1)*(Z2-Z1)
+    double dx2i;                  // 1/(dx*dx) (phisolver_dct)
+    double CFLmax;
+    double M, Vnorm;
+};
+
+// the four viscosity arrays of one time level (cell centres and edges)
+template <typename real>
+struct MuPtrs {
+    const real* cell;
+    const real* xy;
+    const real* xz;
+    const real* yz;
+};
+
 }  // namespace pll

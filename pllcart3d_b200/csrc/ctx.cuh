@@ -1,0 +1,97 @@
+// Device context of the pllcart3d B200 step: the state buffers of both
+// precision forms and the bookkeeping shared by the orchestration units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../include/pllcart3d_gpu.h"
+#include "aux_kernels.cuh"
+#include "common.cuh"
+#include "dct_kernels.cuh"
+#include "host_util.h"
+#include "step_kernels.cuh"
+
+
+namespace pll {
+
+template <typename real>
+struct Bufs {
+    real* q[4][2] = {};     // c, u, v, w : [buffer]
+    real* H[4][2] = {};
+    real* mu[2][4] = {};    // [buffer][cell, xy, xz, yz]
+    real* pg[4] = {};       // u, v, w at 1..3
+    real* phi = nullptr;
+    real* div = nullptr;
+    real* S = nullptr;      // ADI right-hand side / eliminated rhs
+    real* cc = nullptr;     // Thomas scratch
+    real* dct1 = nullptr;   // compact nx*ny*nz Poisson buffers
+    real* dct2 = nullptr;
+    real *Ty = nullptr, *Tz = nullptr, *Tiy = nullptr, *Tiz = nullptr;
+};
+
+}  // namespace pll
+
+using namespace pll;
+
+struct pllgpu_ctx {
+    pllgpu_params P;
+    Geo G;
+    Rng Rg, Rv[4];
+    Consts K;
+    int dev = 0;
+    bool mixed = false;
+    cudaStream_t st = nullptr;
+    long nelem = 0;             // elements of one padded field
+    Bufs<double> b64;           // state of the FP64 form
+    Bufs<float> b32;            // state of the mixed form
+    double *mode_cc = nullptr, *mode_rr = nullptr;  // FP64 Poisson mode scratch
+    double* stage64 = nullptr;  // one padded FP64 field (mixed-form transfers)
+    double *lam_y = nullptr, *lam_z = nullptr;
+    double* scal = nullptr;     // device scalars (S_*)
+    int* status = nullptr;      // device sticky status bits
+    double* work = nullptr;     // slope-parameter scratch
+    double* diag = nullptr;     // per-plane diagnostics + results
+    int cur = 0;                // buffer index holding the "old" role
+    bool rotated = false;       // fast steps ran: "new" roles are stale and
+                                // logically equal to "old" (see materialize)
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    bool graphs_ready = false;
+    double timestep = 0;
+    int err = PLLGPU_OK;
+    int launches_per_step = 0;
+    int counting = 0;
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<const char*> ev_label;
+    std::vector<void*> allocs;
+};
+
+namespace pll {
+
+template <typename real> Bufs<real>& bufs(pllgpu_ctx* c);
+template <> inline Bufs<double>& bufs<double>(pllgpu_ctx* c) { return c->b64; }
+template <> inline Bufs<float>& bufs<float>(pllgpu_ctx* c) { return c->b32; }
+
+template <typename real> real* q_old(pllgpu_ctx* c, int v) { return bufs<real>(c).q[v][c->cur]; }
+template <typename real> real* q_new(pllgpu_ctx* c, int v) { return bufs<real>(c).q[v][1 - c->cur]; }
+template <typename real> real* h_n(pllgpu_ctx* c, int v) { return bufs<real>(c).H[v][1 - c->cur]; }
+template <typename real> real* h_nm1(pllgpu_ctx* c, int v) { return bufs<real>(c).H[v][c->cur]; }
+template <typename real> MuPtrs<real> mu_old(pllgpu_ctx* c)
+{
+    Bufs<real>& B = bufs<real>(c);
+    return {B.mu[c->cur][0], B.mu[c->cur][1], B.mu[c->cur][2], B.mu[c->cur][3]};
+}
+template <typename real> MuPtrs<real> mu_new(pllgpu_ctx* c)
+{
+    Bufs<real>& B = bufs<real>(c);
+    return {B.mu[1 - c->cur][0], B.mu[1 - c->cur][1], B.mu[1 - c->cur][2], B.mu[1 - c->cur][3]};
+}
+
+}  // namespace pll

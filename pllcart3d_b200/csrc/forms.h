@@ -1,0 +1,23 @@
+// Entry points of the two precision forms (form_f64.cu, form_f32.cu).
+#pragma once
+
+struct pllgpu_ctx;
+
+namespace pll {
+
+void form_enqueue_step_f64(pllgpu_ctx* c);
+void form_enqueue_step_f32(pllgpu_ctx* c);
+int form_start_f64(pllgpu_ctx* c);
+int form_start_f32(pllgpu_ctx* c);
+int form_routine_f64(pllgpu_ctx* c, int routine, const double* in, double* out);
+int form_routine_f32(pllgpu_ctx* c, int routine, const double* in, double* out);
+int form_materialize_f64(pllgpu_ctx* c);
+int form_materialize_f32(pllgpu_ctx* c);
+void* form_field_ptr_f64(pllgpu_ctx* c, int f);
+void* form_field_ptr_f32(pllgpu_ctx* c, int f);
+void form_diag_f64(pllgpu_ctx* c);
+void form_diag_f32(pllgpu_ctx* c);
+bool form_alloc_f64(pllgpu_ctx* c);
+bool form_alloc_f32(pllgpu_ctx* c);
+
+}  // namespace pll

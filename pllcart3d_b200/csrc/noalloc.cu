@@ -26,6 +26,7 @@ using namespace pll;
 // part it reads before reading it, so nothing needs clearing.
 static __device__ __align__(256) double g_dct_scratch[PLLGPU_DCT_NOALLOC_MAX_DOUBLES];
 
+namespace pll {
 namespace {
 
 constexpr int kMaxDevices = 64;
@@ -55,6 +56,7 @@ __global__ void k_dct_matrix(int kind, int n, double* T)
 }
 
 }  // namespace
+}  // namespace pll
 
 extern "C" int pllgpu_dct2d_batch_noalloc(int kind, int n0, int n1, int howmany, const double* d_in,
                                           double* d_out, void* stream)

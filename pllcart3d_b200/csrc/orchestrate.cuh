@@ -1,0 +1,533 @@
+// Orchestration of the step (pllcart3d.c:156-196), templated on the storage
+// type: stage launchers, the substep/step sequences, start-up and the
+// per-routine entry points.  form_f64.cu (compiled without multiply-add
+// contraction) and form_f32.cu (with) each instantiate one precision form
+// and export it through the functions declared in forms.h.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "forms.h"
+#include "host_common.cuh"
+
+namespace pll {
+namespace {
+
+// RK3 (Wray) coefficients, global_variables.h:17-18
+const double kRK1[3] = {(8.0 / 15.0), (5.0 / 12.0), (3.0 / 4.0)};
+const double kRK2[3] = {(0.0), (-17.0 / 60.0), (-5.0 / 12.0)};
+
+// ---- stage launchers --------------------------------------------------------
+
+template <typename real, int VAR>
+void launch_explicit(pllgpu_ctx* ctx, const real* un, const real* vn, const real* wn, double g, double r)
+{
+    static const char* lab[4] = {"explicit_c", "explicit_u", "explicit_v", "explicit_w"};
+    const Rng& R = ctx->Rv[VAR];
+    ExplicitArgs<real> A;
+    A.q = q_old<real>(ctx, VAR);
+    A.un = un;
+    A.vn = vn;
+    A.wn = wn;
+    A.mu = mu_old<real>(ctx);
+    A.cn = q_new<real>(ctx, VC);
+    A.pg = VAR == VC ? nullptr : bufs<real>(ctx).pg[VAR];
+    A.Hm = h_nm1<real>(ctx, VAR);
+    A.H = h_n<real>(ctx, VAR);
+    A.S = bufs<real>(ctx).S;
+    A.scal = ctx->scal;
+    A.g = g;
+    A.r = r;
+    A.alpha = g + r;
+    dim3 blk(32, 4);
+    k_explicit<VAR, real><<<box_grid(nk(R), nj(R), ni(R), blk), blk, 0, ctx->st>>>(ctx->G, R, ctx->K, A);
+    mark(ctx, lab[VAR]);
+}
+
+template <typename real, int VAR>
+void launch_implicit(pllgpu_ctx* ctx, double g, double r)
+{
+    static const char* ly[4] = {"adi_y_c", "adi_y_u", "adi_y_v", "adi_y_w"};
+    static const char* lz[4] = {"adi_z_c", "adi_z_u", "adi_z_v", "adi_z_w"};
+    static const char* lx[4] = {"adi_x_c", "adi_x_u", "adi_x_v", "adi_x_w"};
+    const Rng& R = ctx->Rv[VAR];
+    const double alpha = g + r;
+    Bufs<real>& B = bufs<real>(ctx);
+    XsweepArgs<real> X;
+    X.mu = mu_new<real>(ctx);
+    X.q = q_old<real>(ctx, VAR);
+    X.qn = q_new<real>(ctx, VAR);
+    X.H = h_n<real>(ctx, VAR);
+    X.Hm = h_nm1<real>(ctx, VAR);
+    X.S = B.S;
+    X.cc = B.cc;
+    X.scal = ctx->scal;
+    X.g = g;
+    X.r = r;
+    X.alpha = alpha;
+    k_line_pf<VAR, 1, real><<<dim3((nk(R) + 63) / 64, ni(R)), 64, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
+    mark(ctx, ly[VAR]);
+    constexpr size_t smem = adi_z_smem_bytes<VAR, real>();
+    k_adi_z_tiled<VAR, real><<<dim3((nj(R) + 127) / 128, ni(R)), 128, smem, ctx->st>>>(
+        ctx->G, R, ctx->K, X.mu, B.S, B.cc, ctx->scal, alpha);
+    mark(ctx, lz[VAR]);
+    k_line_pf<VAR, 0, real><<<dim3((nk(R) + 63) / 64, nj(R)), 64, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
+    mark(ctx, lx[VAR]);
+}
+
+template <typename real>
+void launch_viscosity(pllgpu_ctx* ctx, const real* cn, MuPtrs<real> m, int law = -1)
+{
+    dim3 blk(32, 4);
+    k_viscosity<real><<<box_grid(ctx->G.NZ, ctx->G.NY, ni(ctx->Rg) + 2, blk), blk, 0, ctx->st>>>(
+        ctx->G, ctx->Rg, ctx->K, law < 0 ? ctx->P.nmvp : law, cn, (real*)m.cell, (real*)m.xy, (real*)m.xz,
+        (real*)m.yz, ctx->scal);
+    mark(ctx, "viscosity");
+}
+
+void launch_gemm(pllgpu_ctx* ctx, const GemmDesc& d, const double* A, const double* B, double* C)
+{
+    dim3 grid((d.N + 63) / 64, (d.M + 63) / 64, d.batch);
+    if (ctx->P.exact_dct)
+        k_gemm_seq<double><<<grid, 256, 0, ctx->st>>>(d, A, B, C);
+    else
+        k_gemm_dmma<<<grid, 256, 0, ctx->st>>>(d, A, B, C);
+    mark(ctx, "dct_gemm");
+}
+
+void launch_gemm(pllgpu_ctx* ctx, const GemmDesc& d, const float* A, const float* B, float* C)
+{
+    dim3 grid((d.N + 63) / 64, (d.M + 63) / 64, d.batch);
+    if (ctx->P.exact_dct)
+        k_gemm_seq<float><<<grid, 256, 0, ctx->st>>>(d, A, B, C);
+    else
+        k_gemm_tf32x3<<<grid, 256, 0, ctx->st>>>(d, A, B, C);
+    mark(ctx, "dct_gemm");
+}
+
+// phisolver_dct after its right-hand side is in dct1 (compact [x][y][z])
+template <typename real>
+void launch_poisson(pllgpu_ctx* ctx)
+{
+    Bufs<real>& B = bufs<real>(ctx);
+    const int nx = ctx->G.nx, ny = ctx->G.ny, nz = ctx->G.nz;
+    const long N = (long)ny * nz;
+    GemmDesc d{};
+    // forward, y pass: dct2[x][ky][z] = sum_y Ty[ky][y] dct1[x][y][z]
+    d = GemmDesc{ny, nz, ny, nx, 0, ny, 1, N, nz, 1, N, nz, 1, 0.0, 0};
+    launch_gemm(ctx, d, B.Ty, B.dct1, B.dct2);
+    // forward, z pass: dct1[x][ky][kz] = sum_z dct2[x][ky][z] Tz[kz][z]
+    d = GemmDesc{ny, nz, nz, nx, N, nz, 1, 0, 1, nz, N, nz, 1, 0.0, 0};
+    launch_gemm(ctx, d, B.dct2, B.Tz, B.dct1);
+    // x-tridiagonal per mode, in place in dct1, FP64 arithmetic
+    k_poisson_x<real><<<(int)((N + 127) / 128), 128, 0, ctx->st>>>(nx, ny, nz, ctx->K, ctx->lam_y, ctx->lam_z,
+                                                                  B.dct1, ctx->mode_cc, ctx->mode_rr);
+    mark(ctx, "poisson_x");
+    // inverse, y pass: dct2[x][y][kz] = sum_ky Tiy[y][ky] dct1[x][ky][kz]
+    d = GemmDesc{ny, nz, ny, nx, 0, ny, 1, N, nz, 1, N, nz, 1, 0.0, 0};
+    launch_gemm(ctx, d, B.Tiy, B.dct1, B.dct2);
+    // inverse, z pass into phi's interior, divided by 4*ny*nz
+    const double four_n = (double)(4 * N);
+    d = GemmDesc{ny, nz, nz, nx, N, nz, 1, 0, 1, nz, ctx->G.sx, ctx->G.sy, 1,
+                 is_pow2(four_n) ? 1.0 / four_n : four_n, is_pow2(four_n) ? 1 : 2};
+    real* phi0 = B.phi + (long)ctx->Rg.is * ctx->G.sx + (long)ctx->Rg.js * ctx->G.sy + ctx->Rg.ks;
+    launch_gemm(ctx, d, B.dct2, B.Tiz, phi0);
+}
+
+template <typename real>
+void launch_phi_ghosts(pllgpu_ctx* ctx)
+{
+    const Rng& R = ctx->Rg;
+    real* phi = bufs<real>(ctx).phi;
+    k_phi_ghosts<0, real><<<dim3((nj(R) + 127) / 128, ni(R)), 128, 0, ctx->st>>>(ctx->G, R, phi);
+    mark(ctx, "phi_ghosts");
+    k_phi_ghosts<1, real><<<dim3((nk(R) + 127) / 128, ni(R)), 128, 0, ctx->st>>>(ctx->G, R, phi);
+    mark(ctx, "phi_ghosts");
+    k_phi_ghosts<2, real><<<dim3((nk(R) + 127) / 128, nj(R)), 128, 0, ctx->st>>>(ctx->G, R, phi);
+    mark(ctx, "phi_ghosts");
+}
+
+template <typename real>
+void launch_project(pllgpu_ctx* ctx, double alpha, int correct, int ghosts, int pgu)
+{
+    Bufs<real>& B = bufs<real>(ctx);
+    ProjectArgs<real> A;
+    A.u = q_new<real>(ctx, VU);
+    A.v = q_new<real>(ctx, VV);
+    A.w = q_new<real>(ctx, VW);
+    A.pgu = B.pg[VU];
+    A.pgv = B.pg[VV];
+    A.pgw = B.pg[VW];
+    A.phi = B.phi;
+    A.mu = mu_new<real>(ctx);
+    A.scal = ctx->scal;
+    A.alpha = alpha;
+    A.do_correct = correct;
+    A.do_ghosts = ghosts;
+    A.do_pg = pgu;
+    dim3 blk(32, 4);
+    k_project<real><<<box_grid(nk(ctx->Rg), nj(ctx->Rg), ni(ctx->Rg) + 1, blk), blk, 0, ctx->st>>>(
+        ctx->G, ctx->Rg, ctx->Rv[VU], ctx->Rv[VV], ctx->Rv[VW], ctx->K, A);
+    mark(ctx, "project");
+}
+
+template <typename real>
+void launch_div(pllgpu_ctx* ctx, int mode, double alpha)
+{
+    Bufs<real>& B = bufs<real>(ctx);
+    dim3 blk(32, 4);
+    k_div_rhs<real><<<box_grid(nk(ctx->Rg), nj(ctx->Rg), ni(ctx->Rg), blk), blk, 0, ctx->st>>>(
+        ctx->G, ctx->Rg, ctx->K, q_new<real>(ctx, VU), q_new<real>(ctx, VV), q_new<real>(ctx, VW), B.div, B.div,
+        B.dct1, ctx->scal, alpha, mode);
+    mark(ctx, "div_rhs");
+}
+
+template <typename real>
+void launch_flux(pllgpu_ctx* ctx)
+{
+    k_flux<real><<<1, 512, sizeof(double) * 2 * ctx->G.NY, ctx->st>>>(ctx->G, ctx->Rv[VU], ctx->K,
+                                                                       q_new<real>(ctx, VU), ctx->scal);
+    mark(ctx, "flux");
+}
+
+template <typename real>
+void launch_bulk(pllgpu_ctx* ctx)
+{
+    k_bulk_velo<real><<<1, 1024, 0, ctx->st>>>(ctx->G, ctx->Rg, q_old<real>(ctx, VU), ctx->scal);
+    mark(ctx, "bulk_velo");
+}
+
+template <typename real>
+void launch_cfl(pllgpu_ctx* ctx)
+{
+    dim3 blk(32, 8);
+    k_cfl<real><<<box_grid(nk(ctx->Rg), nj(ctx->Rg), ni(ctx->Rg), blk), blk, 0, ctx->st>>>(
+        ctx->G, ctx->Rg, ctx->K, q_old<real>(ctx, VU), q_old<real>(ctx, VV), q_old<real>(ctx, VW), ctx->scal,
+        ctx->status);
+    mark(ctx, "cfl");
+    k_dt<<<1, 1, 0, ctx->st>>>(ctx->K, ctx->scal);
+    mark(ctx, "dt");
+}
+
+// one RK3-CN substep of the fast path, pllcart3d.c:164-194
+template <typename real>
+void enqueue_substep(pllgpu_ctx* ctx, int rk)
+{
+    const double g = kRK1[rk], r = kRK2[rk], alpha = g + r;
+    const real *uo = q_old<real>(ctx, VU), *vo = q_old<real>(ctx, VV), *wo = q_old<real>(ctx, VW);
+    launch_bulk<real>(ctx);
+    // concentration: advected by u->new == u->old
+    launch_explicit<real, VC>(ctx, uo, vo, wo, g, r);
+    launch_implicit<real, VC>(ctx, g, r);
+    launch_viscosity<real>(ctx, q_new<real>(ctx, VC), mu_new<real>(ctx));
+    launch_explicit<real, VU>(ctx, uo, vo, wo, g, r);
+    launch_implicit<real, VU>(ctx, g, r);
+    launch_explicit<real, VV>(ctx, uo, vo, wo, g, r);
+    launch_implicit<real, VV>(ctx, g, r);
+    launch_explicit<real, VW>(ctx, uo, vo, wo, g, r);
+    launch_implicit<real, VW>(ctx, g, r);
+    // update_velo_boundary (L182) writes only ghost entries that nothing
+    // reads before update_veloghost_points (L189) rewrites them; skipped
+    launch_flux<real>(ctx);
+    launch_div<real>(ctx, 0, alpha);
+    launch_poisson<real>(ctx);
+    launch_phi_ghosts<real>(ctx);
+    launch_project<real>(ctx, alpha, 1, 1, 1);
+    ctx->cur ^= 1;  // update_old_*: roles swap
+}
+
+__global__ void k_tval(double* scal, double a0, double a1, double a2)
+{
+    // tval += (gamma+rho) dt per substep, pllcart3d.c:166
+    const double dt = scal[S_DT];
+    double t = scal[S_TVAL];
+    t = t + a0 * dt;
+    t = t + a1 * dt;
+    t = t + a2 * dt;
+    scal[S_TVAL] = t;
+}
+
+template <typename real>
+void enqueue_step(pllgpu_ctx* ctx)
+{
+    launch_cfl<real>(ctx);
+    for (int rk = 0; rk < 3; ++rk) enqueue_substep<real>(ctx, rk);
+    k_tval<<<1, 1, 0, ctx->st>>>(ctx->scal, kRK1[0] + kRK2[0], kRK1[1] + kRK2[1], kRK1[2] + kRK2[2]);
+    mark(ctx, "tval");
+}
+
+template <typename real>
+int materialize_t(pllgpu_ctx* ctx)
+{
+    const size_t bytes = sizeof(real) * (size_t)ctx->nelem;
+    Bufs<real>& B = bufs<real>(ctx);
+    for (int v = 0; v < 4; ++v) {
+        CK(cudaMemcpyAsync(q_new<real>(ctx, v), q_old<real>(ctx, v), bytes, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpyAsync(h_n<real>(ctx, v), h_nm1<real>(ctx, v), bytes, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpyAsync(B.mu[1 - ctx->cur][v], B.mu[ctx->cur][v], bytes, cudaMemcpyDeviceToDevice, ctx->st));
+    }
+    return PLLGPU_OK;
+}
+
+template <typename real>
+real* field_ptr_raw(pllgpu_ctx* ctx, int f)
+{
+    if (f < 0 || f >= PLLGPU_NFIELDS) return nullptr;
+    Bufs<real>& B = bufs<real>(ctx);
+    if (f <= PLLGPU_C_HNM1) {
+        const int r = f - PLLGPU_C_OLD;
+        return r == 0 ? q_old<real>(ctx, VC) : r == 1 ? q_new<real>(ctx, VC) : r == 2 ? h_n<real>(ctx, VC)
+                                                                             : h_nm1<real>(ctx, VC);
+    }
+    if (f <= PLLGPU_W_PG) {
+        const int v = 1 + (f - PLLGPU_U_OLD) / 5, r = (f - PLLGPU_U_OLD) % 5;
+        return r == 0 ? q_old<real>(ctx, v) : r == 1 ? q_new<real>(ctx, v) : r == 2 ? h_n<real>(ctx, v)
+             : r == 3 ? h_nm1<real>(ctx, v) : B.pg[v];
+    }
+    if (f <= PLLGPU_MU_OLD_YZ) return B.mu[ctx->cur][f - PLLGPU_MU_OLD_CELL];
+    if (f <= PLLGPU_MU_NEW_YZ) return B.mu[1 - ctx->cur][f - PLLGPU_MU_NEW_CELL];
+    if (f == PLLGPU_PHI) return B.phi;
+    return B.div;
+}
+
+// ---- start-up, routines ---------------------------------------------------------
+
+template <typename real>
+int start_t(pllgpu_ctx* ctx)
+{
+    const size_t bytes = sizeof(real) * (size_t)ctx->nelem;
+    // update_ghost_points (L81) on the initial velocities; phi is zero
+    launch_project<real>(ctx, 0.0, 0, 1, 0);
+    // update_old_conc / update_old_velo (L82-83): both buffers equal
+    for (int v = 0; v < 4; ++v) {
+        CK(cudaMemcpyAsync(q_old<real>(ctx, v), q_new<real>(ctx, v), bytes, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpyAsync(h_nm1<real>(ctx, v), h_n<real>(ctx, v), bytes, cudaMemcpyDeviceToDevice, ctx->st));
+    }
+    if (ctx->P.nmvp) {
+        const double PI = 4.0 * std::atan(1.0);
+        // slope_parameter reads FP64 c (pllcart3d.c:133); the mixed form
+        // widens its FP32 c through the staging field
+        const double* c64 = nullptr;
+        if (ctx->mixed) {
+            k_convert_to_f64<<<(int)((ctx->nelem + 255) / 256), 256, 0, ctx->st>>>(
+                ctx->nelem, (const float*)q_new<real>(ctx, VC), ctx->stage64);
+            c64 = ctx->stage64;
+        } else {
+            c64 = (const double*)q_new<real>(ctx, VC);
+        }
+        k_slope_parameter<<<1, 1, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->P.Y1, ctx->P.Z1, ctx->G.dy, ctx->G.dz,
+                                                ctx->P.Vratio, ctx->P.Mum, ctx->P.Lambda, PI, c64, ctx->scal,
+                                                ctx->status, ctx->work);
+    }
+    // calculate_viscosity(c->old, mu_old), L142
+    launch_viscosity<real>(ctx, q_old<real>(ctx, VC), mu_old<real>(ctx));
+    return PLLGPU_OK;
+}
+
+int set_dt_vb(pllgpu_ctx* ctx, double dt, double vb)
+{
+    if (set_scalar(ctx, S_DT, dt) || set_scalar(ctx, S_VBULK, vb)) return ctx->err;
+    return PLLGPU_OK;
+}
+
+template <typename real>
+int routine_t(pllgpu_ctx* ctx, int routine, const double* in, double* out)
+{
+    const double dt = in ? in[0] : 0.0, g = in ? in[1] : 0.0, r = in ? in[2] : 0.0, vb = in ? in[3] : 0.0;
+    const double alpha = g + r;
+    const size_t bytes = sizeof(real) * (size_t)ctx->nelem;
+    Bufs<real>& B = bufs<real>(ctx);
+    switch (routine) {
+    case PLLGPU_R_CONCENTRATION:
+        if (set_dt_vb(ctx, dt, vb)) return ctx->err;
+        launch_explicit<real, VC>(ctx, q_new<real>(ctx, VU), q_new<real>(ctx, VV), q_new<real>(ctx, VW), g, r);
+        launch_implicit<real, VC>(ctx, g, r);
+        break;
+    case PLLGPU_R_VISCOSITY_NEW:
+        launch_viscosity<real>(ctx, q_new<real>(ctx, VC), mu_new<real>(ctx));
+        break;
+    case PLLGPU_R_XMOM:
+    case PLLGPU_R_YMOM:
+    case PLLGPU_R_ZMOM: {
+        if (set_dt_vb(ctx, dt, vb)) return ctx->err;
+        const real *uo = q_old<real>(ctx, VU), *vo = q_old<real>(ctx, VV), *wo = q_old<real>(ctx, VW);
+        if (routine == PLLGPU_R_XMOM) {
+            launch_explicit<real, VU>(ctx, uo, vo, wo, g, r);
+            launch_implicit<real, VU>(ctx, g, r);
+        } else if (routine == PLLGPU_R_YMOM) {
+            launch_explicit<real, VV>(ctx, uo, vo, wo, g, r);
+            launch_implicit<real, VV>(ctx, g, r);
+        } else {
+            launch_explicit<real, VW>(ctx, uo, vo, wo, g, r);
+            launch_implicit<real, VW>(ctx, g, r);
+        }
+        break;
+    }
+    case PLLGPU_R_VELO_GHOSTS:
+        launch_project<real>(ctx, 0.0, 0, 1, 0);
+        break;
+    case PLLGPU_R_DIVERGENCE:
+        launch_div<real>(ctx, 1, 0.0);
+        break;
+    case PLLGPU_R_PHISOLVER:
+        if (set_scalar(ctx, S_DT, dt)) return ctx->err;
+        launch_div<real>(ctx, 2, alpha);
+        launch_poisson<real>(ctx);
+        break;
+    case PLLGPU_R_PHI_GHOSTS:
+        launch_phi_ghosts<real>(ctx);
+        break;
+    case PLLGPU_R_VELO_CORRECTION:
+        if (set_scalar(ctx, S_DT, dt)) return ctx->err;
+        launch_flux<real>(ctx);
+        launch_project<real>(ctx, alpha, 1, 0, 0);
+        break;
+    case PLLGPU_R_PRESSURE_GRADIENT:
+        if (set_scalar(ctx, S_DT, dt)) return ctx->err;
+        launch_project<real>(ctx, alpha, 0, 0, 1);
+        break;
+    case PLLGPU_R_ROTATE:
+        for (int v = 0; v < 4; ++v) {
+            CK(cudaMemcpyAsync(q_old<real>(ctx, v), q_new<real>(ctx, v), bytes, cudaMemcpyDeviceToDevice, ctx->st));
+            CK(cudaMemcpyAsync(h_nm1<real>(ctx, v), h_n<real>(ctx, v), bytes, cudaMemcpyDeviceToDevice, ctx->st));
+            CK(cudaMemcpyAsync(B.mu[ctx->cur][v], B.mu[1 - ctx->cur][v], bytes, cudaMemcpyDeviceToDevice, ctx->st));
+        }
+        break;
+    case PLLGPU_R_BULK_VELO:
+        launch_bulk<real>(ctx);
+        if (out) out[0] = get_scalar(ctx, S_VBULK);
+        break;
+    case PLLGPU_R_FIND_CFL:
+        // find_cfl's own return value CFLmax/max (before the Timestep clip)
+        launch_cfl<real>(ctx);
+        if (out) out[0] = get_scalar(ctx, S_CFLDT);
+        break;
+    case PLLGPU_R_SUBSTEP: {
+        const int rk = (int)g;
+        if (rk < 0 || rk > 2) return fail(ctx, PLLGPU_EINVAL);
+        if (set_scalar(ctx, S_DT, dt)) return ctx->err;
+        enqueue_substep<real>(ctx, rk);
+        ctx->rotated = true;
+        break;
+    }
+    case PLLGPU_R_VISCOSITY_EXP:
+        launch_viscosity<real>(ctx, q_new<real>(ctx, VC), mu_new<real>(ctx), 0);
+        break;
+    case PLLGPU_R_VISCOSITY_NMVP: {
+        // coefficients of calculate_viscosity_nmvp (pllcart3d.c:895-900)
+        const double cm = dt, PI = 4.0 * std::atan(1.0), M = ctx->P.Vratio;
+        const double alp = std::exp(M), mum = ctx->P.Mum * alp;
+        const double psi0 = std::asin(alp / mum), psi1 = PI - std::asin(1 / mum);
+        const double etam = (PI / 2 - psi0) / (psi1 - psi0);
+        const double a = ((1 - cm) - etam) / ((1 - cm) * (etam - 1));
+        if (set_scalar(ctx, S_CM, cm) || set_scalar(ctx, S_MUM, mum) || set_scalar(ctx, S_PSI0, psi0) ||
+            set_scalar(ctx, S_PSI1, psi1) || set_scalar(ctx, S_NMVA, a))
+            return ctx->err;
+        launch_viscosity<real>(ctx, q_new<real>(ctx, VC), mu_new<real>(ctx), 1);
+        break;
+    }
+    case PLLGPU_R_SLOPE_PARAMETER: {
+        if (ctx->mixed) return fail(ctx, PLLGPU_EINVAL);
+        const double PI = 4.0 * std::atan(1.0);
+        k_slope_parameter<<<1, 1, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->P.Y1, ctx->P.Z1, ctx->G.dy, ctx->G.dz,
+                                                ctx->P.Vratio, ctx->P.Mum, ctx->P.Lambda, PI,
+                                                (const double*)q_new<real>(ctx, VC), ctx->scal, ctx->status,
+                                                ctx->work);
+        mark(ctx, "slope_parameter");
+        if (out) out[0] = get_scalar(ctx, S_CM);
+        break;
+    }
+    default:
+        return fail(ctx, PLLGPU_EINVAL);
+    }
+    return PLLGPU_OK;
+}
+
+// FP64 diagnostics: mass, divergence norms, mixing length
+__global__ void k_diag_final(int nplanes, int ny, int nz, double dV, double dx, const double* __restrict__ pl,
+                             double* __restrict__ out)
+{
+    double mass = 0.0, dmax = 0.0, d2 = 0.0, lmix = 0.0;
+    for (int i = 0; i < nplanes; ++i) {
+        const double sc = pl[3 * i], cbar = sc / ((double)ny * (double)nz);
+        mass += sc * dV;
+        dmax = fmax(dmax, pl[3 * i + 1]);
+        d2 += pl[3 * i + 2];
+        if (cbar > 0.01 && cbar < 0.99) lmix += dx;
+    }
+    out[0] = mass;
+    out[1] = dmax;
+    out[2] = sqrt(d2 * dV);
+    out[3] = lmix;
+}
+
+template <typename real>
+void launch_diag(pllgpu_ctx* ctx)
+{
+    const Rng& R = ctx->Rg;
+    k_plane_diag<real><<<ni(R), 256, 0, ctx->st>>>(ctx->G, R, ctx->K, q_old<real>(ctx, VC), q_old<real>(ctx, VU),
+                                                   q_old<real>(ctx, VV), q_old<real>(ctx, VW), ctx->diag);
+    const double dV = ctx->G.dx * ctx->G.dy * ctx->G.dz;
+    k_diag_final<<<1, 1, 0, ctx->st>>>(ni(R), ctx->G.ny, ctx->G.nz, dV, ctx->G.dx, ctx->diag,
+                                       ctx->diag + 3L * ni(R));
+}
+
+template <typename real>
+bool alloc_state(pllgpu_ctx* c)
+{
+    Bufs<real>& B = bufs<real>(c);
+    const pllgpu_params* p = &c->P;
+    bool ok = true;
+    for (int v = 0; v < 4 && ok; ++v)
+        for (int b = 0; b < 2 && ok; ++b)
+            ok = (B.q[v][b] = dalloc<real>(c, c->nelem)) && (B.H[v][b] = dalloc<real>(c, c->nelem));
+    for (int b = 0; b < 2 && ok; ++b)
+        for (int m = 0; m < 4 && ok; ++m) ok = (B.mu[b][m] = dalloc<real>(c, c->nelem)) != nullptr;
+    for (int v = 1; v < 4 && ok; ++v) ok = (B.pg[v] = dalloc<real>(c, c->nelem)) != nullptr;
+    const long ncell = (long)p->nx * p->ny * p->nz;
+    ok = ok && (B.phi = dalloc<real>(c, c->nelem)) && (B.div = dalloc<real>(c, c->nelem)) &&
+         (B.S = dalloc<real>(c, c->nelem)) && (B.cc = dalloc<real>(c, c->nelem)) &&
+         (B.dct1 = dalloc<real>(c, ncell)) && (B.dct2 = dalloc<real>(c, ncell)) &&
+         (B.Ty = dalloc<real>(c, (long)p->ny * p->ny)) && (B.Tz = dalloc<real>(c, (long)p->nz * p->nz)) &&
+         (B.Tiy = dalloc<real>(c, (long)p->ny * p->ny)) && (B.Tiz = dalloc<real>(c, (long)p->nz * p->nz));
+    if (!ok) return false;
+    std::vector<real> T((size_t)std::max(p->ny, p->nz) * std::max(p->ny, p->nz));
+    dct_matrix<real>(0, p->ny, T.data());
+    cudaMemcpy(B.Ty, T.data(), sizeof(real) * p->ny * p->ny, cudaMemcpyHostToDevice);
+    dct_matrix<real>(0, p->nz, T.data());
+    cudaMemcpy(B.Tz, T.data(), sizeof(real) * p->nz * p->nz, cudaMemcpyHostToDevice);
+    dct_matrix<real>(1, p->ny, T.data());
+    cudaMemcpy(B.Tiy, T.data(), sizeof(real) * p->ny * p->ny, cudaMemcpyHostToDevice);
+    dct_matrix<real>(1, p->nz, T.data());
+    cudaMemcpy(B.Tiz, T.data(), sizeof(real) * p->nz * p->nz, cudaMemcpyHostToDevice);
+    // kernels above the 48 KB default of dynamic shared memory
+    cudaFuncSetAttribute(k_adi_z_tiled<VC, real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)adi_z_smem_bytes<VC, real>());
+    cudaFuncSetAttribute(k_adi_z_tiled<VU, real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)adi_z_smem_bytes<VU, real>());
+    cudaFuncSetAttribute(k_adi_z_tiled<VV, real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)adi_z_smem_bytes<VV, real>());
+    cudaFuncSetAttribute(k_adi_z_tiled<VW, real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)adi_z_smem_bytes<VW, real>());
+    return true;
+}
+
+}  // namespace
+}  // namespace pll
+
+// exported entry points of one precision form
+#define PLL_DEFINE_FORM(SUFFIX, REAL)                                                          \
+    namespace pll {                                                                          \
+    void form_enqueue_step_##SUFFIX(pllgpu_ctx* c) { enqueue_step<REAL>(c); }                \
+    int form_start_##SUFFIX(pllgpu_ctx* c) { return start_t<REAL>(c); }                      \
+    int form_routine_##SUFFIX(pllgpu_ctx* c, int r, const double* in, double* out)           \
+    {                                                                                        \
+        return routine_t<REAL>(c, r, in, out);                                               \
+    }                                                                                        \
+    int form_materialize_##SUFFIX(pllgpu_ctx* c) { return materialize_t<REAL>(c); }          \
+    void* form_field_ptr_##SUFFIX(pllgpu_ctx* c, int f) { return (void*)field_ptr_raw<REAL>(c, f); } \
+    void form_diag_##SUFFIX(pllgpu_ctx* c) { launch_diag<REAL>(c); }                         \
+    bool form_alloc_##SUFFIX(pllgpu_ctx* c) { return alloc_state<REAL>(c); }                 \
+    }

@@ -12,29 +12,9 @@
 #include "common.cuh"
 
 namespace pll {
-
-// ---------------------------------------------------------------------------
-// constants shared by the stencil kernels (host-precomputed, exact as in the
-// reference: each is the same IEEE expression the reference evaluates)
-// ---------------------------------------------------------------------------
-struct Consts {
-    double hx, hy, hz;            // dx, dy, dz
-    double ihx, ihy, ihz;         // 1/dx ... (used only when pow2)
-    double i2hx, i2hy, i2hz;      // 1/(2 dx) ... (used only when pow2)
-    int pow2;                     // all spacings are exact powers of two
-    double cdx, cdy, cdz;         // 1/(Pe h^2), A_conc (pllcart3d.c:1421-1433)
-    double d1x, d1y, d1z;         // 1/(Re h)
-    double d2x, d2y, d2z;         // 2/(Re h)
-    double xuv, xuw;              // 1/(Re dy dx), 1/(Re dz dx)  (Hu_op)
-    double xvu, xvw;              // 1/(Re dx dy), 1/(Re dz dy)  (Hv_op)
-    double xwu, xwv;              // 1/(Re dx dz), 1/(Re dy dz)  (Hw_op)
-    double FxRe, FyRe;            // -(Fx/Re), -(Fy/Re)
-    double Re;
-    double area;                  // (Y2-Y1)*(Z2-Z1)
-    double dx2i;                  // 1/(dx*dx) (phisolver_dct)
-    double CFLmax;
-    double M, Vnorm;
-};
+// internal linkage: each translation unit (and so each precision form with
+// its own contraction flags) owns its instantiations
+namespace {
 
 enum { MU_CELL_ = 0, MU_XY_ = 1, MU_XZ_ = 2, MU_YZ_ = 3 };
 
@@ -98,7 +78,10 @@ __device__ __forceinline__ real weno5(real v0, real v1, real v2, real v3, real v
     t1 = (real)1.0 * v2 - (real)2.0 * v3 + v4;
     t2 = (real)3.0 * v2 - (real)4.0 * v3 + v4;
     real s3 = (con2 * t1 * t1) + (con3 * t2 * t2);
-    real eps = (real)1.0e-6 * maxd + (real)1.0e-99;
+    // FP64: the reference's 1e-99 floor.  FP32: 1e-99 underflows to 0 and
+    // (s+eps)^2 could be 0; 1e-18 keeps (s+eps)^2 >= 1e-36, a normal float,
+    // and below any smoothness indicator that matters
+    real eps = (real)1.0e-6 * maxd + (sizeof(real) == 8 ? (real)1.0e-99 : (real)1.0e-18);
     real a1 = (real)0.1 / ((s1 + eps) * (s1 + eps));
     real a2 = (real)0.6 / ((s2 + eps) * (s2 + eps));
     real a3 = (real)0.3 / ((s3 + eps) * (s3 + eps));
@@ -231,14 +214,6 @@ __device__ __forceinline__ void acoef(const Consts& K, const Geo& G,
     }
     b = -(a + c);
 }
-
-template <typename real>
-struct MuPtrs {
-    const real* cell;
-    const real* xy;
-    const real* xz;
-    const real* yz;
-};
 
 template <typename real>
 struct ExplicitArgs {
@@ -892,4 +867,5 @@ __global__ void __launch_bounds__(128) k_line_pf(Geo G, Rng R, Consts K, XsweepA
     }
 }
 
+}  // namespace
 }  // namespace pll

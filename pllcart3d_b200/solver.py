@@ -26,9 +26,16 @@ def _dp(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
+PRECISIONS = {"fp64": 0, "mixed": 1}
+
+
 class Solver:
+    """precision="fp64": the reference's FP64 arithmetic; "mixed": FP32 state
+    and stencils, split-TF32 tensor-core DCT, FP64 Poisson mode solve and
+    reductions."""
+
     def __init__(self, params: Params, device: int = 0, exact_dct: bool = False,
-                 use_graph: bool = True):
+                 use_graph: bool = True, precision: str = "fp64"):
         params.validate()
         self.params = params
         L = _lib.lib()
@@ -40,7 +47,8 @@ class Solver:
         p.Re, p.Pe, p.Vratio = params.Re, params.Pe, params.Vratio
         p.Fx, p.Fy, p.CFLmax = params.Fx, params.Fy, params.CFLmax
         p.Timestep, p.Mum, p.Lambda = params.Timestep, params.Mum, params.Lambda
-        p.precision = 0
+        p.precision = PRECISIONS[precision]
+        self.precision = precision
         p.exact_dct = int(bool(exact_dct))
         p.use_graph = int(bool(use_graph))
         self._L = L
@@ -114,6 +122,12 @@ class Solver:
     @property
     def kernels_per_step(self) -> int:
         return self._L.pllgpu_kernels_per_step(self._h)
+
+    def diagnostics(self) -> dict:
+        """FP64 mass, max |div u|, L2 |div u| and mixing length of the state."""
+        out = (ctypes.c_double * 4)()
+        self._check(self._L.pllgpu_diagnostics(self._h, out), "diagnostics")
+        return {"mass": out[0], "div_max": out[1], "div_l2": out[2], "mixing_length": out[3]}
 
     def status(self) -> int:
         return self._L.pllgpu_status(self._h)
