@@ -60,7 +60,10 @@ typedef struct pllgpu_params {
     int exact_dct;         /* 1: DCT sums in sequential order (bitwise with
                               the CPU restatement); 0: tensor-core DMMA        */
     int use_graph;         /* 1: replay each step as one CUDA graph            */
-    int reserved[5];
+    int dct_kernel;        /* precision form, exact_dct 0: 0 = tcgen05 split-TF32
+                              GEMMs where ny, nz are 128 or 256, else mma.sync;
+                              1 = mma.sync split-TF32 always                   */
+    int reserved[4];
 } pllgpu_params;
 
 typedef struct pllgpu_ctx pllgpu_ctx;

@@ -36,7 +36,7 @@ CU_SOURCES = {"runtime.cu": "--fmad=false", "form_f64.cu": "--fmad=false",
               "form_f32.cu": "--fmad=true", "primitives.cu": "--fmad=false",
               "noalloc.cu": "--fmad=false"}
 HEADERS = ["common.cuh", "step_kernels.cuh", "aux_kernels.cuh", "dct_kernels.cuh", "host_util.h",
-           "ctx.cuh", "host_common.cuh", "orchestrate.cuh", "forms.h"]
+           "ctx.cuh", "host_common.cuh", "orchestrate.cuh", "forms.h", "umma_dct.cuh"]
 
 
 def _nvcc() -> str:

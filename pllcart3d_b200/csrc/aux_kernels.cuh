@@ -230,11 +230,12 @@ __global__ void __launch_bounds__(128) k_poisson_x(int nx, int ny, int nz, Const
                                                    const double* __restrict__ lam_y,
                                                    const double* __restrict__ lam_z,
                                                    T* __restrict__ hat, double* __restrict__ cc,
-                                                   double* __restrict__ rr)
+                                                   double* __restrict__ rr, int kz_major = 0)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ny * nz) return;
-    const int jy = t / nz, kz = t % nz;
+    // modes stored [x][ky][kz] (kz_major 0) or [x][kz][ky] (kz_major 1)
+    const int jy = kz_major ? t % ny : t / nz, kz = kz_major ? t / ny : t % nz;
     const long st = (long)ny * nz;
     const double a = K.dx2i, c = K.dx2i;
     const double bmid = -2.0 * K.dx2i + lam_y[jy] + lam_z[kz];

@@ -54,6 +54,7 @@ enum StatusBits {
     ST_NAN = 1,       // a NaN/Inf met in the CFL scan
     ST_NOCONV = 2,    // slope-parameter bisection did not converge
     ST_BOUNDS = 4,    // a kernel's self-check found a bad index
+    ST_TIMEOUT = 8,   // a bounded device wait ran out
 };
 
 // ---------------------------------------------------------------------------

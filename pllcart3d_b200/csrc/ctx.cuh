@@ -2,6 +2,7 @@
 // precision forms and the bookkeeping shared by the orchestration units.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -36,6 +37,15 @@ struct Bufs {
     real *Ty = nullptr, *Tz = nullptr, *Tiy = nullptr, *Tiz = nullptr;
 };
 
+// tcgen05 DCT passes of the precision form: tensor maps of the four passes
+// (A = the data, Bh / Bl = the cosine matrix's TF32 head and tail)
+struct UmmaPlan {
+    bool on = false;
+    CUtensorMap a[4], bh[4], bl[4];
+    float* Thi[4] = {};
+    float* Tlo[4] = {};
+};
+
 }  // namespace pll
 
 using namespace pll;
@@ -54,6 +64,7 @@ struct pllgpu_ctx {
     double *mode_cc = nullptr, *mode_rr = nullptr;  // FP64 Poisson mode scratch
     double* stage64 = nullptr;  // one padded FP64 field (mixed-form transfers)
     double *lam_y = nullptr, *lam_z = nullptr;
+    UmmaPlan um;                // precision form's tensor-core DCT (when shapes allow)
     double* scal = nullptr;     // device scalars (S_*)
     int* status = nullptr;      // device sticky status bits
     double* work = nullptr;     // slope-parameter scratch

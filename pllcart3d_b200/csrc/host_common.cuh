@@ -96,6 +96,7 @@ int read_status(pllgpu_ctx* ctx)
     if (s & ST_NAN) return fail(ctx, PLLGPU_ENAN);
     if (s & ST_NOCONV) return fail(ctx, PLLGPU_ENOCONV);
     if (s & ST_BOUNDS) return fail(ctx, PLLGPU_EBOUNDS);
+    if (s & ST_TIMEOUT) return fail(ctx, PLLGPU_ETIMEOUT);
     return PLLGPU_OK;
 }
 

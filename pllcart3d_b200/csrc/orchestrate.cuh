@@ -7,10 +7,14 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
+
+#include <type_traits>
 
 #include "forms.h"
 #include "host_common.cuh"
+#include "umma_dct.cuh"
 
 namespace pll {
 namespace {
@@ -107,10 +111,54 @@ void launch_gemm(pllgpu_ctx* ctx, const GemmDesc& d, const float* A, const float
     mark(ctx, "dct_gemm");
 }
 
+// one tcgen05 DCT pass over all planes (pass 0 forward z, 1 forward y,
+// 2 inverse y, 3 inverse z); rows = planes x rows per plane, K = the
+// transform length = the output columns
+void launch_umma(pllgpu_ctx* ctx, int pass, long rows, int K, const UmmaEpi& e, float* out)
+{
+    const UmmaPlan& U = ctx->um;
+    const dim3 grid((unsigned)(rows / UM_BM));
+    if (K == 256)
+        k_dct_umma<256><<<grid, UM_THREADS, UmmaSmem<256>::DYN, ctx->st>>>(U.a[pass], U.bh[pass], U.bl[pass], K, e,
+                                                                           out, ctx->status);
+    else
+        k_dct_umma<128><<<grid, UM_THREADS, UmmaSmem<128>::DYN, ctx->st>>>(U.a[pass], U.bh[pass], U.bl[pass], K, e,
+                                                                           out, ctx->status);
+    mark(ctx, "dct_umma");
+}
+
+void launch_poisson_umma(pllgpu_ctx* ctx)
+{
+    Bufs<float>& B = ctx->b32;
+    const int nx = ctx->G.nx, ny = ctx->G.ny, nz = ctx->G.nz;
+    const long N = (long)ny * nz;
+    // forward z: dct2[x][kz][y] = sum_z dct1[x][y][z] Tz[kz][z] (stored transposed)
+    launch_umma(ctx, 0, (long)nx * ny, nz, UmmaEpi{ny, N, 1, ny, 1.f, 0, 1}, B.dct2);
+    // forward y: dct1[x][kz][ky] = sum_y dct2[x][kz][y] Ty[ky][y]
+    launch_umma(ctx, 1, (long)nx * nz, ny, UmmaEpi{nz, N, ny, 1, 1.f, 0, 0}, B.dct1);
+    k_poisson_x<float><<<(int)((N + 127) / 128), 128, 0, ctx->st>>>(nx, ny, nz, ctx->K, ctx->lam_y, ctx->lam_z,
+                                                                   B.dct1, ctx->mode_cc, ctx->mode_rr, 1);
+    mark(ctx, "poisson_x");
+    // inverse y: dct2[x][y][kz] = sum_ky dct1[x][kz][ky] Tiy[y][ky] (stored transposed)
+    launch_umma(ctx, 2, (long)nx * nz, ny, UmmaEpi{nz, N, 1, nz, 1.f, 0, 1}, B.dct2);
+    // inverse z into phi's interior, divided by 4*ny*nz
+    const double four_n = (double)(4 * N);
+    const bool p2 = is_pow2(four_n);
+    float* phi0 = B.phi + (long)ctx->Rg.is * ctx->G.sx + (long)ctx->Rg.js * ctx->G.sy + ctx->Rg.ks;
+    launch_umma(ctx, 3, (long)nx * ny, nz,
+                UmmaEpi{ny, ctx->G.sx, ctx->G.sy, 1, (float)(p2 ? 1.0 / four_n : four_n), p2 ? 1 : 2, 0}, phi0);
+}
+
 // phisolver_dct after its right-hand side is in dct1 (compact [x][y][z])
 template <typename real>
 void launch_poisson(pllgpu_ctx* ctx)
 {
+    if constexpr (std::is_same<real, float>::value) {
+        if (ctx->um.on) {
+            launch_poisson_umma(ctx);
+            return;
+        }
+    }
     Bufs<real>& B = bufs<real>(ctx);
     const int nx = ctx->G.nx, ny = ctx->G.ny, nz = ctx->G.nz;
     const long N = (long)ny * nz;
@@ -474,6 +522,85 @@ void launch_diag(pllgpu_ctx* ctx)
                                        ctx->diag + 3L * ni(R));
 }
 
+// ---- tcgen05 DCT set-up (precision form) ----------------------------------------
+
+// TF32 round-to-nearest, ties away from zero, of a finite float
+float tf32_rna_host(float x)
+{
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    u = (u + 0x1000u) & ~0x1FFFu;
+    float r;
+    std::memcpy(&r, &u, 4);
+    return r;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// row-major FP32 matrix [rows][cols], boxes of 32 columns x box_rows rows,
+// 128-byte swizzle (the shared-memory layout tcgen05 reads as K-major SW128)
+bool tile_map(CUtensorMap* m, const float* base, long rows, int cols, int box_rows)
+{
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn || ((uintptr_t)base & 15) || (cols * 4) % 16 || cols % UM_BK || box_rows > 256) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)cols * 4};
+    const cuuint32_t box[2] = {(cuuint32_t)UM_BK, (cuuint32_t)box_rows};
+    const cuuint32_t es[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)base, dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool setup_umma(pllgpu_ctx* c)
+{
+    Bufs<float>& B = c->b32;
+    UmmaPlan& U = c->um;
+    const int nx = c->P.nx, ny = c->P.ny, nz = c->P.nz;
+    // pass: A buffer, A rows, transform length, cosine matrix (FP32, [n][k])
+    const float* A[4] = {B.dct1, B.dct2, B.dct1, B.dct2};
+    const long rows[4] = {(long)nx * ny, (long)nx * nz, (long)nx * nz, (long)nx * ny};
+    const int len[4] = {nz, ny, ny, nz};
+    const float* T[4] = {B.Tz, B.Ty, B.Tiy, B.Tiz};
+    for (int p = 0; p < 4; ++p) {
+        const long n2 = (long)len[p] * len[p];
+        std::vector<float> t((size_t)n2), hi((size_t)n2), lo((size_t)n2);
+        if (cudaMemcpy(t.data(), T[p], sizeof(float) * n2, cudaMemcpyDeviceToHost) != cudaSuccess) return false;
+        for (long i = 0; i < n2; ++i) {
+            hi[i] = tf32_rna_host(t[i]);
+            lo[i] = tf32_rna_host(t[i] - hi[i]);
+        }
+        if (!(U.Thi[p] = dalloc<float>(c, n2)) || !(U.Tlo[p] = dalloc<float>(c, n2))) return false;
+        cudaMemcpy(U.Thi[p], hi.data(), sizeof(float) * n2, cudaMemcpyHostToDevice);
+        cudaMemcpy(U.Tlo[p], lo.data(), sizeof(float) * n2, cudaMemcpyHostToDevice);
+        if (!tile_map(&U.a[p], A[p], rows[p], len[p], UM_BM) || !tile_map(&U.bh[p], U.Thi[p], len[p], len[p], len[p]) ||
+            !tile_map(&U.bl[p], U.Tlo[p], len[p], len[p], len[p]))
+            return false;
+    }
+    if (cudaFuncSetAttribute(k_dct_umma<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)UmmaSmem<256>::DYN) != cudaSuccess ||
+        cudaFuncSetAttribute(k_dct_umma<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)UmmaSmem<128>::DYN) != cudaSuccess)
+        return false;
+    U.on = true;
+    return true;
+}
+
 template <typename real>
 bool alloc_state(pllgpu_ctx* c)
 {
@@ -511,6 +638,10 @@ bool alloc_state(pllgpu_ctx* c)
                          (int)adi_z_smem_bytes<VV, real>());
     cudaFuncSetAttribute(k_adi_z_tiled<VW, real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)adi_z_smem_bytes<VW, real>());
+    if constexpr (std::is_same<real, float>::value) {
+        const bool shape_ok = (p->ny == 128 || p->ny == 256) && (p->nz == 128 || p->nz == 256);
+        if (shape_ok && !p->exact_dct && p->dct_kernel == 0 && !setup_umma(c)) return false;
+    }
     return true;
 }
 

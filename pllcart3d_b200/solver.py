@@ -32,10 +32,12 @@ PRECISIONS = {"fp64": 0, "mixed": 1}
 class Solver:
     """precision="fp64": the reference's FP64 arithmetic; "mixed": FP32 state
     and stencils, split-TF32 tensor-core DCT, FP64 Poisson mode solve and
-    reductions."""
+    reductions.  dct_kernel="auto" runs the precision form's DCT passes as
+    tcgen05 GEMMs where the plane shape allows (ny, nz in {128, 256}),
+    "mma_sync" keeps the warp-level split-TF32 GEMM."""
 
     def __init__(self, params: Params, device: int = 0, exact_dct: bool = False,
-                 use_graph: bool = True, precision: str = "fp64"):
+                 use_graph: bool = True, precision: str = "fp64", dct_kernel: str = "auto"):
         params.validate()
         self.params = params
         L = _lib.lib()
@@ -51,6 +53,7 @@ class Solver:
         self.precision = precision
         p.exact_dct = int(bool(exact_dct))
         p.use_graph = int(bool(use_graph))
+        p.dct_kernel = {"auto": 0, "mma_sync": 1}[dct_kernel]
         self._L = L
         self._h = L.pllgpu_create(ctypes.byref(p), int(device))
         if not self._h:
