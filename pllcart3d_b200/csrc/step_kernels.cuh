@@ -18,10 +18,31 @@ namespace {
 
 enum { MU_CELL_ = 0, MU_XY_ = 1, MU_XZ_ = 2, MU_YZ_ = 3 };
 
+// x / h as the reference divides; exact as x * (1/h) when h is a power of
+// two.  The precision form (FP32) always multiplies by the rounded 1/h.
 template <typename real>
 __device__ __forceinline__ real over_h(real x, double h, double ih, int pow2)
 {
     return pow2 ? x * (real)ih : x / (real)h;
+}
+
+template <>
+__device__ __forceinline__ float over_h<float>(float x, double, double ih, int)
+{
+    return x * (float)ih;
+}
+
+// x / (2 h), the ENO-2 second difference
+template <typename real>
+__device__ __forceinline__ real over_2h(real x, double h, double i2h, int pow2)
+{
+    return pow2 ? x * (real)i2h : x / ((real)2.0 * (real)h);
+}
+
+template <>
+__device__ __forceinline__ float over_2h<float>(float x, double, double i2h, int)
+{
+    return x * (float)i2h;
 }
 
 // advecting velocity of variable VAR for the pass along AXIS at point id
@@ -89,6 +110,33 @@ __device__ __forceinline__ real weno5(real v0, real v1, real v2, real v3, real v
     return (a1 / at) * c1 + (a2 / at) * c2 + (a3 / at) * c3;
 }
 
+// The precision form's WENO5: the same weights with four approximate
+// divisions (__fdividef, <= 2 ulp) in place of six IEEE ones.  With the FP32
+// floor eps >= 1e-18 every (s+eps)^2 lies in [1e-36, 2^126), where
+// __fdividef is accurate, and so does the weight sum.
+template <>
+__device__ __forceinline__ float weno5<float>(float v0, float v1, float v2, float v3, float v4)
+{
+    const float con1 = (float)(1.0 / 6.0), con2 = (float)(13.0 / 12.0), con3 = 0.25f;
+    const float maxd = fmaxf(fmaxf(fmaxf(v0 * v0, v1 * v1), fmaxf(v2 * v2, v3 * v3)), v4 * v4);
+    const float c1 = con1 * (2.0f * v0 - 7.0f * v1 + 11.0f * v2);
+    const float c2 = con1 * (-v1 + 5.0f * v2 + 2.0f * v3);
+    const float c3 = con1 * (2.0f * v2 + 5.0f * v3 - v4);
+    float t1 = v0 - 2.0f * v1 + v2, t2 = v0 - 4.0f * v1 + 3.0f * v2;
+    const float s1 = con2 * t1 * t1 + con3 * t2 * t2;
+    t1 = v1 - 2.0f * v2 + v3;
+    t2 = v1 - v3;
+    const float s2 = con2 * t1 * t1 + con3 * t2 * t2;
+    t1 = v2 - 2.0f * v3 + v4;
+    t2 = 3.0f * v2 - 4.0f * v3 + v4;
+    const float s3 = con2 * t1 * t1 + con3 * t2 * t2;
+    const float eps = 1.0e-6f * maxd + 1.0e-18f;
+    const float a1 = __fdividef(0.1f, (s1 + eps) * (s1 + eps));
+    const float a2 = __fdividef(0.6f, (s2 + eps) * (s2 + eps));
+    const float a3 = __fdividef(0.3f, (s3 + eps) * (s3 + eps));
+    return __fdividef(a1 * c1 + a2 * c2 + a3 * c3, a1 + a2 + a3);
+}
+
 // D2 value an earlier directional pass of the same H*_op call left in its
 // scratch line at index m (pllcart3d.c:1545-1546: D1/D2 are allocated once
 // per call, zeroed, and reused by the x, y and z passes; each pass writes
@@ -111,7 +159,7 @@ __device__ real stale_d2(const real* __restrict__ q, const Geo& G, const Rng& R,
             }
             real d1m = over_h<real>(q[base + (long)(m + 1) * st] - q[base + (long)m * st], h, ih, K.pow2);
             real d1p = over_h<real>(q[base + (long)m * st] - q[base + (long)(m - 1) * st], h, ih, K.pow2);
-            return K.pow2 ? (d1m - d1p) * (real)i2h : (d1m - d1p) / ((real)2.0 * (real)h);
+            return over_2h<real>(d1m - d1p, h, i2h, K.pow2);
         }
     }
     return (real)0;
@@ -139,28 +187,30 @@ __device__ __forceinline__ real upwind_deriv(const real* __restrict__ q, const G
         real d2a, d2b;
         if (kk >= s) {
             real d1m = over_h<real>(q[b] - q[b - st], h, ih, K.pow2);
-            d2a = K.pow2 ? (d1k - d1m) * (real)i2h : (d1k - d1m) / ((real)2.0 * (real)h);
+            d2a = over_2h<real>(d1k - d1m, h, i2h, K.pow2);
         } else {
             d2a = stale_d2<real>(q, G, R, K, AXIS, kk);
         }
         if (kk + 1 <= e) {
             real d1p = over_h<real>(q[b + 2 * st] - q[b + st], h, ih, K.pow2);
-            d2b = K.pow2 ? (d1p - d1k) * (real)i2h : (d1p - d1k) / ((real)2.0 * (real)h);
+            d2b = over_2h<real>(d1p - d1k, h, i2h, K.pow2);
         } else {
             d2b = stale_d2<real>(q, G, R, K, AXIS, kk + 1);
         }
         real d2v = (fabs(d2a) <= fabs(d2b)) ? d2a : d2b;
         return d1k + d2v * (real)h * (real)sign;
     }
-    // WENO: D1[kk + sign*t], t = 0..4, kk = m-3 (sign>0) or m+2 (sign<0)
-    const int kk = m - 3 - (int)(2.5 * (sign - 1));
-    real v[5];
+    // WENO: D1[kk + sign*t], t = 0..4, kk = m-3 (sign>0) or m+2 (sign<0).
+    // Both windows lie in D1[m-3 .. m+2]: form those six differences from
+    // q[m-3 .. m+3] at fixed offsets and pick the window by the sign.
+    real d[6];
 #pragma unroll
-    for (int t = 0; t < 5; ++t) {
-        const long p = id + (long)(kk + sign * t - m) * st;
-        v[t] = over_h<real>(q[p + st] - q[p], h, ih, K.pow2);
+    for (int t = 0; t < 6; ++t) {
+        const long p = id + (long)(t - 3) * st;
+        d[t] = over_h<real>(q[p + st] - q[p], h, ih, K.pow2);
     }
-    return weno5<real>(v[0], v[1], v[2], v[3], v[4]);
+    const bool up = sign == 1;
+    return weno5<real>(up ? d[0] : d[5], up ? d[1] : d[4], up ? d[2] : d[3], up ? d[3] : d[2], up ? d[4] : d[1]);
 }
 
 // implicit-operator coefficients (A_conc/A_umom/A_vmom/A_wmom,
@@ -303,12 +353,12 @@ __global__ void __launch_bounds__(128) k_explicit(Geo G, Rng R, Consts K,
         real bf;
         if (VAR == VU) {
             real cval = (real)0.5 * (A.cn[id] + A.cn[id - sx]);
-            bf = alpha * ((real)K.FxRe * cval - (A.pg[id] / (real)K.Re));
+            bf = alpha * ((real)K.FxRe * cval - over_h<real>(A.pg[id], K.Re, 1.0 / K.Re, 0));
         } else if (VAR == VV) {
             real cval = (real)0.5 * (A.cn[id] + A.cn[id - sy]);
-            bf = alpha * ((real)K.FyRe * cval - (A.pg[id] / (real)K.Re));
+            bf = alpha * ((real)K.FyRe * cval - over_h<real>(A.pg[id], K.Re, 1.0 / K.Re, 0));
         } else {
-            bf = alpha * (-(A.pg[id] / (real)K.Re));
+            bf = alpha * (-over_h<real>(A.pg[id], K.Re, 1.0 / K.Re, 0));
         }
         S = dt * (conv + diff + bf);
     }
