@@ -240,37 +240,82 @@ __global__ void __launch_bounds__(128) k_poisson_x(int nx, int ny, int nz, Const
     const double a = K.dx2i, c = K.dx2i;
     const double bmid = -2.0 * K.dx2i + lam_y[jy] + lam_z[kz];
     const bool gauge = (jy == 0) && (kz == 0);
+    // the loads of PF positions ahead are issued before the recurrence
+    // consumes the current ones (the line is strided by ny*nz)
+    constexpr int PF = 8;
     double cprev = 0, rprev = 0;
-    for (int m = 0; m < nx; ++m) {
-        const long id = t + (long)m * st;
-        double lb = bmid, lr = (double)hat[id];
-        if (m == 0) lb += a;
-        if (m == nx - 1) {
-            if (gauge) lr -= c * 0.0;
-            else lb += c;
+    T hv[PF];
+#pragma unroll
+    for (int u = 0; u < PF; ++u) hv[u] = u < nx ? hat[t + (long)u * st] : (T)0;
+    for (int m0 = 0; m0 < nx; m0 += PF) {
+        T hn[PF];
+#pragma unroll
+        for (int u = 0; u < PF; ++u) {
+            const int m = m0 + PF + u;
+            hn[u] = m < nx ? hat[t + (long)m * st] : (T)0;
         }
-        double cm, rm;
-        if (m == 0) {
-            lb = lb - 0.0 * a;
-            cm = c / lb;
-            rm = (lr - 0.0 * a) / lb;
-        } else {
-            lb = (lb - cprev * a);
-            cm = c / lb;
-            rm = (lr - rprev * a) / lb;
+#pragma unroll
+        for (int u = 0; u < PF; ++u) {
+            const int m = m0 + u;
+            if (m < nx) {
+                const long id = t + (long)m * st;
+                double lb = bmid, lr = (double)hv[u];
+                if (m == 0) lb += a;
+                if (m == nx - 1) {
+                    if (gauge) lr -= c * 0.0;
+                    else lb += c;
+                }
+                double cm, rm;
+                if (m == 0) {
+                    lb = lb - 0.0 * a;
+                    cm = c / lb;
+                    rm = (lr - 0.0 * a) / lb;
+                } else {
+                    lb = (lb - cprev * a);
+                    cm = c / lb;
+                    rm = (lr - rprev * a) / lb;
+                }
+                cc[id] = cm;
+                rr[id] = rm;
+                cprev = cm;
+                rprev = rm;
+            }
         }
-        cc[id] = cm;
-        rr[id] = rm;
-        cprev = cm;
-        rprev = rm;
+#pragma unroll
+        for (int u = 0; u < PF; ++u) hv[u] = hn[u];
     }
     double xnext = rprev - cprev * 0.0;
     hat[t + (long)(nx - 1) * st] = (T)xnext;
-    for (int m = nx - 2; m >= 0; --m) {
-        const long id = t + (long)m * st;
-        double x = rr[id] - cc[id] * xnext;
-        hat[id] = (T)x;
-        xnext = x;
+    double rv[PF], cv[PF];
+    int mtop = nx - 2;
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+        const int m = mtop - u;
+        rv[u] = m >= 0 ? rr[t + (long)m * st] : 0.0;
+        cv[u] = m >= 0 ? cc[t + (long)m * st] : 0.0;
+    }
+    for (; mtop >= 0; mtop -= PF) {
+        double rn[PF], cn[PF];
+#pragma unroll
+        for (int u = 0; u < PF; ++u) {
+            const int m = mtop - PF - u;
+            rn[u] = m >= 0 ? rr[t + (long)m * st] : 0.0;
+            cn[u] = m >= 0 ? cc[t + (long)m * st] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < PF; ++u) {
+            const int m = mtop - u;
+            if (m >= 0) {
+                const double x = rv[u] - cv[u] * xnext;
+                hat[t + (long)m * st] = (T)x;
+                xnext = x;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < PF; ++u) {
+            rv[u] = rn[u];
+            cv[u] = cn[u];
+        }
     }
 }
 

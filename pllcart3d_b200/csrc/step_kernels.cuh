@@ -165,6 +165,24 @@ __device__ real stale_d2(const real* __restrict__ q, const Geo& G, const Rng& R,
     return (real)0;
 }
 
+// c' = c / b', r' = r / b' of one Thomas step.  The precision form
+// multiplies by one approximate reciprocal (b' >= 1 for these diagonally
+// dominant systems, so __fdividef is accurate to 2 ulp).
+template <typename real>
+__device__ __forceinline__ void thomas_div(real lc, real num, real bb, real& cm, real& rm)
+{
+    cm = lc / bb;
+    rm = num / bb;
+}
+
+template <>
+__device__ __forceinline__ void thomas_div<float>(float lc, float num, float bb, float& cm, float& rm)
+{
+    const float ib = __fdividef(1.0f, bb);
+    cm = lc * ib;
+    rm = num * ib;
+}
+
 // upwind derivative of q along AXIS at point id (line position m); the
 // ENO-2 closure on the first and last two points of the range, WENO5
 // elsewhere (e.g. Hc_op pllcart3d.c:1553-1576)
@@ -430,12 +448,10 @@ __global__ void __launch_bounds__(128) k_adi_yz(Geo G, Rng R, Consts K, MuPtrs<r
         real bb, cm, rm;
         if (m == 0) {
             bb = lb;
-            cm = lc / bb;
-            rm = lr / bb;
+            thomas_div<real>(lc, lr, bb, cm, rm);
         } else {
             bb = lb - cprev * la;
-            cm = lc / bb;
-            rm = (lr - rprev * la) / bb;
+            thomas_div<real>(lc, (lr - rprev * la), bb, cm, rm);
         }
         cc[id] = cm;
         S[id] = rm;
@@ -505,12 +521,10 @@ __global__ void __launch_bounds__(128) k_adi_x(Geo G, Rng R, Consts K, XsweepArg
         real cm, rm;
         if (m == 0) {
             lb = lb - (real)0.0 * la;
-            cm = lc / lb;
-            rm = (lr - (real)0.0 * la) / lb;
+            thomas_div<real>(lc, (lr - (real)0.0 * la), lb, cm, rm);
         } else {
             lb = (lb - cprev * la);
-            cm = lc / lb;
-            rm = (lr - rprev * la) / lb;
+            thomas_div<real>(lc, (lr - rprev * la), lb, cm, rm);
         }
         A.cc[id] = cm;
         A.S[id] = rm;
@@ -561,29 +575,32 @@ __global__ void __launch_bounds__(128) k_adi_x(Geo G, Rng R, Consts K, XsweepArg
 // ---------------------------------------------------------------------------
 // ADI line solve along z (the contiguous axis), same arithmetic as
 // k_adi_yz<VAR,2>, but each warp owns 32 neighbouring lines (fixed i,
-// consecutive j) and moves them through shared memory in 32x32 tiles, so
-// that every global access is a coalesced 256-byte row segment instead of 32
-// lines' worth of strided ones.  Forward elimination writes c' to `cc` and
-// the eliminated rhs over S, tile by tile; back substitution walks the tiles
-// in reverse.
+// consecutive j) and moves them through shared memory in tiles of 32 lines x
+// ZW positions, so that every global access is a coalesced row segment
+// instead of 32 lines' worth of strided ones.  Forward elimination writes c'
+// to `cc` and the eliminated rhs over S, tile by tile; back substitution
+// walks the tiles in reverse.  The recurrence is latency-bound (one
+// dependent chain per lane), so the tiles are kept narrow (ZW = 16) to
+// leave room for twice the resident warps that hide it.
 // ---------------------------------------------------------------------------
+constexpr int ZW = 16;
+
 template <int VAR, typename real>
 constexpr size_t adi_z_smem_bytes()
 {
-    return sizeof(real) * 4 * 32 * (2 * 33 + (VAR == VC ? 0 : 34));
+    // per warp: S and c' tiles [32][ZW+1], viscosity tile [32][ZW+3]
+    return sizeof(real) * 4 * 32 * (2 * (ZW + 1) + (VAR == VC ? 0 : ZW + 3));
 }
 
 template <int VAR, typename real>
-__global__ void __launch_bounds__(128) k_adi_z_tiled(Geo G, Rng R, Consts K, MuPtrs<real> mu,
+__global__ void __launch_bounds__(128, 4) k_adi_z_tiled(Geo G, Rng R, Consts K, MuPtrs<real> mu,
                                                      real* __restrict__ S, real* __restrict__ cc,
                                                      const double* __restrict__ scal, double alpha)
 {
     constexpr int W = 32;
-    // dynamic shared memory: per warp an S tile, a c' tile and (momentum) a
-    // viscosity tile; adi_z_smem_bytes() gives the size
     extern __shared__ __align__(16) unsigned char zsm[];
-    typedef real Tile[W][W + 1];
-    typedef real MTile[W][W + 2];
+    typedef real Tile[W][ZW + 1];
+    typedef real MTile[W][ZW + 3];
     Tile* tS = (Tile*)zsm;
     Tile* tC = tS + 4;
     MTile* tM = (MTile*)(tC + 4);
@@ -599,18 +616,56 @@ __global__ void __launch_bounds__(128) k_adi_z_tiled(Geo G, Rng R, Consts K, MuP
     const int moff = VAR == VW ? -1 : 0;
     const double dz_coef = VAR == VW ? K.d2z : K.d1z;
     const long base0 = (long)i * G.sx + (long)j0 * G.sy + R.ks;
+    // tile moves: two rows per warp instruction (lanes 0-15 row r, 16-31
+    // row r+1).  The next tile's loads go to registers before the current
+    // tile's sequential solve, so global latency overlaps the recurrence.
+    constexpr int NR = W / 2;
+    const int hr = lane >> 4, col = lane & (ZW - 1);
+    real pS[NR], pM[NR], pE;
+    // 32-bit offsets from the warp's first row (a plane of a field is far
+    // below 2^31 elements)
+    const int sy = (int)G.sy;
+    auto fetch_fwd = [&](int k0) {
+        const int nk = (n - k0) < ZW ? (n - k0) : ZW;
+        const real* Sb = S + base0 + k0;
+        const real* Mb = mz + base0 + k0 + moff;
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+            const int r = 2 * q + hr;
+            const bool ok = r < nl && col < nk;
+            pS[q] = ok ? Sb[r * sy + col] : (real)0;
+            if (VAR != VC) pM[q] = ok ? Mb[r * sy + col] : (real)0;
+        }
+        // the viscosity value one past the tile, lane = row
+        if (VAR != VC) pE = lane < nl ? Mb[lane * sy + nk] : (real)0;
+    };
+    auto fetch_bwd = [&](int k0) {
+        const int nk = (n - k0) < ZW ? (n - k0) : ZW;
+        const real* Sb = S + base0 + k0;
+        const real* Cb = cc + base0 + k0;
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+            const int r = 2 * q + hr;
+            const bool ok = r < nl && col < nk;
+            pS[q] = ok ? Sb[r * sy + col] : (real)0;
+            pM[q] = ok ? Cb[r * sy + col] : (real)0;
+        }
+    };
     real cprev = 0, rprev = 0;
-    for (int k0 = 0; k0 < n; k0 += W) {
-        const int nk = (n - k0) < W ? (n - k0) : W;
-        for (int r = 0; r < nl; ++r) {
-            const long b = base0 + (long)r * G.sy + k0;
-            if (lane < nk) tS[warp][r][lane] = S[b + lane];
-            if (VAR != VC) {
-                if (lane < nk) tM[warp][r][lane] = mz[b + moff + lane];
-                if (lane == 0) tM[warp][r][nk] = mz[b + moff + nk];
+    fetch_fwd(0);
+    for (int k0 = 0; k0 < n; k0 += ZW) {
+        const int nk = (n - k0) < ZW ? (n - k0) : ZW;
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+            const int r = 2 * q + hr;
+            if (r < nl && col < nk) {
+                tS[warp][r][col] = pS[q];
+                if (VAR != VC) tM[warp][r][col] = pM[q];
             }
         }
+        if (VAR != VC && lane < nl) tM[warp][lane][nk] = pE;
         __syncwarp();
+        if (k0 + ZW < n) fetch_fwd(k0 + ZW);
         if (lane < nl) {
             for (int t = 0; t < nk; ++t) {
                 const int m = k0 + t;
@@ -637,12 +692,10 @@ __global__ void __launch_bounds__(128) k_adi_z_tiled(Geo G, Rng R, Consts K, MuP
                 real bb, cm, rm;
                 if (m == 0) {
                     bb = lb;
-                    cm = lc / bb;
-                    rm = lr / bb;
+                    thomas_div<real>(lc, lr, bb, cm, rm);
                 } else {
                     bb = lb - cprev * la;
-                    cm = lc / bb;
-                    rm = (lr - rprev * la) / bb;
+                    thomas_div<real>(lc, (lr - rprev * la), bb, cm, rm);
                 }
                 tC[warp][lane][t] = cm;
                 tS[warp][lane][t] = rm;
@@ -651,28 +704,33 @@ __global__ void __launch_bounds__(128) k_adi_z_tiled(Geo G, Rng R, Consts K, MuP
             }
         }
         __syncwarp();
-        for (int r = 0; r < nl; ++r) {
-            const long b = base0 + (long)r * G.sy + k0;
-            if (lane < nk) {
-                S[b + lane] = tS[warp][r][lane];
-                cc[b + lane] = tC[warp][r][lane];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+            const int r = 2 * q + hr;
+            if (r < nl && col < nk) {
+                S[base0 + k0 + r * sy + col] = tS[warp][r][col];
+                cc[base0 + k0 + r * sy + col] = tC[warp][r][col];
             }
         }
         __syncwarp();
     }
-    // back substitution, last tile first; x_{n-1} = r'_{n-1}
+    // back substitution, last tile first; x_{n-1} = r'_{n-1}.  Every tile's
+    // S and c' were stored by this warp above (same lanes, same addresses).
     real xnext = rprev;
-    const int last0 = ((n - 1) / W) * W;
-    for (int k0 = last0; k0 >= 0; k0 -= W) {
-        const int nk = (n - k0) < W ? (n - k0) : W;
-        for (int r = 0; r < nl; ++r) {
-            const long b = base0 + (long)r * G.sy + k0;
-            if (lane < nk) {
-                tS[warp][r][lane] = S[b + lane];
-                tC[warp][r][lane] = cc[b + lane];
+    const int last0 = ((n - 1) / ZW) * ZW;
+    fetch_bwd(last0);
+    for (int k0 = last0; k0 >= 0; k0 -= ZW) {
+        const int nk = (n - k0) < ZW ? (n - k0) : ZW;
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+            const int r = 2 * q + hr;
+            if (r < nl && col < nk) {
+                tS[warp][r][col] = pS[q];
+                tC[warp][r][col] = pM[q];
             }
         }
         __syncwarp();
+        if (k0 - ZW >= 0) fetch_bwd(k0 - ZW);
         if (lane < nl) {
             for (int t = nk - 1; t >= 0; --t) {
                 const int m = k0 + t;
@@ -683,9 +741,10 @@ __global__ void __launch_bounds__(128) k_adi_z_tiled(Geo G, Rng R, Consts K, MuP
             }
         }
         __syncwarp();
-        for (int r = 0; r < nl; ++r) {
-            const long b = base0 + (long)r * G.sy + k0;
-            if (lane < nk) S[b + lane] = tS[warp][r][lane];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+            const int r = 2 * q + hr;
+            if (r < nl && col < nk) S[base0 + k0 + r * sy + col] = tS[warp][r][col];
         }
         __syncwarp();
     }
@@ -813,21 +872,17 @@ __global__ void __launch_bounds__(128) k_line_pf(Geo G, Rng R, Consts K, XsweepA
                 if (AXIS == 0) {
                     if (m == 0) {
                         lb = lb - (real)0.0 * la;
-                        cm = lc / lb;
-                        rm = (lr - (real)0.0 * la) / lb;
+                        thomas_div<real>(lc, (lr - (real)0.0 * la), lb, cm, rm);
                     } else {
                         lb = (lb - cprev * la);
-                        cm = lc / lb;
-                        rm = (lr - rprev * la) / lb;
+                        thomas_div<real>(lc, (lr - rprev * la), lb, cm, rm);
                     }
                 } else {
                     if (m == 0) {
-                        cm = lc / lb;
-                        rm = lr / lb;
+                        thomas_div<real>(lc, lr, lb, cm, rm);
                     } else {
                         const real bb = lb - cprev * la;
-                        cm = lc / bb;
-                        rm = (lr - rprev * la) / bb;
+                        thomas_div<real>(lc, (lr - rprev * la), bb, cm, rm);
                     }
                 }
                 const long id = base + (long)m * st;
@@ -844,11 +899,38 @@ __global__ void __launch_bounds__(128) k_line_pf(Geo G, Rng R, Consts K, XsweepA
         }
     }
 
+    // q_new at line position id; for c also its Neumann ghosts in y
+    // (pllcart3d.c:700-705) then z (L707-712), written as the value is
+    // produced.  The z copies run over j in [js-1, je+1] in the reference,
+    // so its corners copy the y ghosts, which equal this line's value.
+    const int jl = R.js + o;
+    const bool jlo = AXIS == 0 && VAR == VC && jl == R.js, jhi = AXIS == 0 && VAR == VC && jl == R.je;
+    const bool klo = AXIS == 0 && VAR == VC && k == R.ks, khi = AXIS == 0 && VAR == VC && k == R.ke;
+    const bool edge = jlo | jhi | klo | khi;
+    auto put = [&](long id, real v) {
+        A.qn[id] = v;
+        if (edge) {
+            const long sy = G.sy;
+            if (jlo) A.qn[id - sy] = v;
+            if (jhi) A.qn[id + sy] = v;
+            if (klo) {
+                A.qn[id - 1] = v;
+                if (jlo) A.qn[id - sy - 1] = v;
+                if (jhi) A.qn[id + sy - 1] = v;
+            }
+            if (khi) {
+                A.qn[id + 1] = v;
+                if (jlo) A.qn[id - sy + 1] = v;
+                if (jhi) A.qn[id + sy + 1] = v;
+            }
+        }
+    };
+
     // back substitution, x_{n-1} = r'_{n-1} (pll form: minus c' * 0)
     real xnext = AXIS == 0 ? rprev - cprev * (real)0.0 : rprev;
     if (AXIS == 0) {
         const long id = base + (long)(n - 1) * st;
-        A.qn[id] = A.q[id] + xnext;
+        put(id, A.q[id] + xnext);
     }
     // positions n-2 .. 0 in chunks of PF, loads of the next chunk first
     real rv[PF], cv[PF], qv[PF];
@@ -877,7 +959,7 @@ __global__ void __launch_bounds__(128) k_line_pf(Geo G, Rng R, Consts K, XsweepA
             if (m >= 0) {
                 const long id = base + (long)m * st;
                 real x = AXIS == 0 ? rv[t] - cv[t] * xnext : rv[t] - xnext * cv[t];
-                if (AXIS == 0) A.qn[id] = qv[t] + x;
+                if (AXIS == 0) put(id, qv[t] + x);
                 else S[id] = x;
                 xnext = x;
             }
@@ -890,31 +972,6 @@ __global__ void __launch_bounds__(128) k_line_pf(Geo G, Rng R, Consts K, XsweepA
         }
     }
 
-    if (AXIS == 0 && VAR == VC) {
-        // Neumann ghosts of c (pllcart3d.c:700-712), as in k_adi_x
-        const long sy = G.sy;
-        const int j = R.js + o;
-        const bool jlo = (j == R.js), jhi = (j == R.je);
-        const bool klo = (k == R.ks), khi = (k == R.ke);
-        if (jlo | jhi | klo | khi) {
-            for (int m = 0; m < n; ++m) {
-                const long id = base + (long)m * st;
-                const real v = A.qn[id];
-                if (jlo) A.qn[id - sy] = v;
-                if (jhi) A.qn[id + sy] = v;
-                if (klo) {
-                    A.qn[id - 1] = v;
-                    if (jlo) A.qn[id - sy - 1] = v;
-                    if (jhi) A.qn[id + sy - 1] = v;
-                }
-                if (khi) {
-                    A.qn[id + 1] = v;
-                    if (jlo) A.qn[id - sy + 1] = v;
-                    if (jhi) A.qn[id + sy + 1] = v;
-                }
-            }
-        }
-    }
 }
 
 }  // namespace
