@@ -119,6 +119,10 @@ int pllgpu_device_field(pllgpu_ctx *ctx, int field, double **dptr,
  * (ghost fill, new -> old), 126-148 (viscosity of c_old, slope parameter)
  * and 150-154 (diffusive cap of Timestep) */
 int pllgpu_start(pllgpu_ctx *ctx);
+/* start-up after pllgpu_read_restart (pllcart3d.c:111 then 126-154): the
+ * viscosity of c_old (and the slope parameter, which the reference computes
+ * from c->new), no ghost fill, no new -> old copy; tval as read */
+int pllgpu_resume(pllgpu_ctx *ctx, double tval);
 /* n full time steps, pllcart3d.c:158-195, dt from the device CFL scan */
 int pllgpu_steps(pllgpu_ctx *ctx, int nsteps);
 /* n steps, copying the four initial fields in from host and c,u,v,w out to
@@ -206,6 +210,43 @@ int pllgpu_dct2d_batch(int kind, int n0, int n1, int howmany, const double *in,
  * threads) race; each call overwrites what it reads, so none needs it
  * cleared.
  */
+/* ---- snapshot, restart and diagnostic files ---------------------------- *
+ * The reference's output routines on the resident state, writing its file
+ * formats into `dir` (NULL: the working directory).  The device packs each
+ * file's values, one copy brings them to pinned host memory.
+ *   pllgpu_write_snapshot  write_to_file (pllcart3d.c:3047): caf%04dR000.bin,
+ *                          float32 u,v,w (cell centres), c per interior cell;
+ *                          only even (i,j,k) cells above 2e7 cells
+ *   pllgpu_write_snapshot_ex  the same with the MPI rank of the file name and
+ *                          subsample -1 (the reference's rule), 0 (all cells)
+ *                          or 1 (even cells)
+ *   pllgpu_write_restart   midfield (L3121): middata + midfield000.bin
+ *   pllgpu_read_restart    intermediate (L3181): reads them into the 14
+ *                          fields; follow with pllgpu_resume
+ *   pllgpu_conc_average    conc_average (L3635): appends cavgy.bin,
+ *                          cavgz.bin, cavgyz.bin
+ *   pllgpu_find_wmax       find_wmax (L3606): appends (wmax, tval) to
+ *                          wmax.bin when dir is given; wmax to *wmax_out
+ *   pllgpu_find_max        find_max (L3539): appends the max |u|,|v|,|w|,|c|
+ *                          block to Outscreen; maxval[4] / maxloc[12] out;
+ *                          a NaN in c (old, new, explicit) writes the
+ *                          reference's "nan in" line and returns PLLGPU_ENAN
+ *                          where the reference calls exit(1)
+ */
+int pllgpu_write_snapshot(pllgpu_ctx *ctx, int fileno, const char *dir);
+int pllgpu_write_snapshot_ex(pllgpu_ctx *ctx, int fileno, int rank,
+                             const char *dir, int subsample);
+int pllgpu_write_restart(pllgpu_ctx *ctx, int tstep, int fileno, double tval,
+                         double outtime, double outmid, double cavgtime,
+                         const char *dir);
+int pllgpu_read_restart(pllgpu_ctx *ctx, const char *dir, int *tstep,
+                        int *fileno, double *tval, double *outtime);
+int pllgpu_conc_average(pllgpu_ctx *ctx, double tval, const char *dir);
+int pllgpu_find_wmax(pllgpu_ctx *ctx, double tval, const char *dir,
+                     double *wmax_out);
+int pllgpu_find_max(pllgpu_ctx *ctx, const char *dir, double *maxval,
+                    int *maxloc);
+
 #define PLLGPU_DCT_NOALLOC_MAX_DOUBLES (1L << 21)
 int pllgpu_dct2d_batch_noalloc(int kind, int n0, int n1, int howmany,
                                const double *d_in, double *d_out,

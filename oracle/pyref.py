@@ -108,6 +108,34 @@ class RefRun:
     def state(self) -> dict:
         return {f: self.get(f) for f in FIELDS}
 
+    # ---- the reference's own output routines, writing into `directory` ----
+    def write_to_file(self, fileno: int, directory: str) -> None:
+        assert self.lib.pllref_write_to_file(int(fileno), directory.encode()) == 0
+
+    def midfield(self, tstep, fileno, tval, outtime, outmid, cavgtime, directory: str) -> None:
+        f = self.lib.pllref_midfield
+        f.argtypes = [_I, _I, _D, _D, _D, _D, ctypes.c_char_p]
+        assert f(int(tstep), int(fileno), tval, outtime, outmid, cavgtime, directory.encode()) == 0
+
+    def intermediate(self, directory: str) -> dict:
+        ts, fn, tv, ot = _I(), _I(), _D(), _D()
+        assert self.lib.pllref_intermediate(directory.encode(), ctypes.byref(ts), ctypes.byref(fn),
+                                            ctypes.byref(tv), ctypes.byref(ot)) == 0
+        return {"tstep": ts.value, "fileno": fn.value, "tval": tv.value, "outtime": ot.value}
+
+    def conc_average(self, tval: float, directory: str) -> None:
+        f = self.lib.pllref_conc_average
+        f.argtypes = [_D, ctypes.c_char_p]
+        assert f(tval, directory.encode()) == 0
+
+    def find_wmax(self, tval: float, directory: str) -> None:
+        f = self.lib.pllref_find_wmax
+        f.argtypes = [_D, ctypes.c_char_p]
+        assert f(tval, directory.encode()) == 0
+
+    def find_max(self, directory: str) -> None:
+        assert self.lib.pllref_find_max(directory.encode()) == 0
+
     @property
     def dt(self) -> float:
         return self.lib.pllref_last_dt()

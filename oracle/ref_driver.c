@@ -79,6 +79,12 @@ void update_old_conc(Conc *);
 void update_old_velo(Velo *, Velo *, Velo *);
 void update_old_visc(Visc *, Visc *);
 void pll_shim_fftw_set_fast(int);
+void write_to_file(int, Grid *, double ***, double ***, double ***, double ***);
+void midfield(int, int, double, double, double, double, Grid *, Conc *, Velo *, Velo *, Velo *);
+void intermediate(int *, int *, double *, double *, Grid *, Conc *, Velo *, Velo *, Velo *);
+void conc_average(Grid *, double ***, double);
+void find_wmax(double, Grid *, Velo *);
+void find_max(Grid *, Velo *, Velo *, Velo *, Conc *);
 
 static Grid *g_grid;
 static Velo *g_u, *g_v, *g_w;
@@ -244,6 +250,31 @@ int pllref_load_ic(const double *c, const double *u, const double *v,
     diff_dt = 0.1 * Pe * del_min * del_min;
     Timestep = (diff_dt < Timestep) ? diff_dt : Timestep;
     g_tval = 0.0;
+    if (chdir(here) != 0) return -1;
+    return 0;
+}
+
+/* pllcart3d.c:126-154 after intermediate() (L111) restored the state */
+int pllref_restart_startup(double tval)
+{
+    double del_min, diff_dt;
+    char here[4096];
+    if (!getcwd(here, sizeof(here)) || chdir(g_rundir) != 0) return -1;
+    if (Nmvp == 1) {
+        g_cm = slope_parameter(g_grid, g_c->new);
+        calculate_viscosity_nmvp(g_grid, g_c->old, g_mu_old, g_cm);
+    } else {
+        calculate_viscosity(g_grid, g_c->old, g_mu_old);
+    }
+    A_conc(g_grid, g_c);
+    A_umom(g_grid, g_mu_old, g_u);
+    A_vmom(g_grid, g_mu_old, g_v);
+    A_wmom(g_grid, g_mu_old, g_w);
+    del_min = (g_grid->dx < g_grid->dy) ? g_grid->dx : g_grid->dy;
+    del_min = (del_min < g_grid->dz) ? del_min : g_grid->dz;
+    diff_dt = 0.1 * Pe * del_min * del_min;
+    Timestep = (diff_dt < Timestep) ? diff_dt : Timestep;
+    g_tval = tval;
     if (chdir(here) != 0) return -1;
     return 0;
 }
@@ -452,3 +483,62 @@ void pllref_structs(void **out)
 }
 
 void pllref_set_tval(double t) { g_tval = t; }
+
+/* ---- the reference's own output routines, run in `dir` ------------------
+ * write_to_file pllcart3d.c:3047, midfield L3121, intermediate L3181,
+ * conc_average L3635, find_wmax L3606, find_max L3539 (whose NaN branch
+ * calls exit(1); callers only use it on finite states). */
+static int in_dir(const char *dir, char *here)
+{
+    if (!getcwd(here, 4096)) return -1;
+    return chdir(dir);
+}
+
+int pllref_write_to_file(int fileno, const char *dir)
+{
+    char here[4096];
+    if (in_dir(dir, here)) return -1;
+    write_to_file(fileno, g_grid, g_u->new, g_v->new, g_w->new, g_c->new);
+    return chdir(here);
+}
+
+int pllref_midfield(int tstep, int fileno, double tval, double outtime, double outmid, double cavgtime,
+                    const char *dir)
+{
+    char here[4096];
+    if (in_dir(dir, here)) return -1;
+    midfield(tstep, fileno, tval, outtime, outmid, cavgtime, g_grid, g_c, g_u, g_v, g_w);
+    return chdir(here);
+}
+
+int pllref_intermediate(const char *dir, int *tstep, int *fileno, double *tval, double *outtime)
+{
+    char here[4096];
+    if (in_dir(dir, here)) return -1;
+    intermediate(tstep, fileno, tval, outtime, g_grid, g_c, g_u, g_v, g_w);
+    return chdir(here);
+}
+
+int pllref_conc_average(double tval, const char *dir)
+{
+    char here[4096];
+    if (in_dir(dir, here)) return -1;
+    conc_average(g_grid, g_c->new, tval);
+    return chdir(here);
+}
+
+int pllref_find_wmax(double tval, const char *dir)
+{
+    char here[4096];
+    if (in_dir(dir, here)) return -1;
+    find_wmax(tval, g_grid, g_w);
+    return chdir(here);
+}
+
+int pllref_find_max(const char *dir)
+{
+    char here[4096];
+    if (in_dir(dir, here)) return -1;
+    find_max(g_grid, g_u, g_v, g_w, g_c);
+    return chdir(here);
+}

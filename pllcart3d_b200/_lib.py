@@ -111,6 +111,15 @@ def lib():
     L.pllgpu_tridiag_1rhs_batch.argtypes = [_I, _I, _PD, _PD, _PD, _PD]
     L.pllgpu_idct2d_batch.argtypes = [_I, _I, _I, _PD, _PD]
     L.pllgpu_dct2d_batch_noalloc.argtypes = [_I, _I, _I, _I, _VP, _VP, _VP]
+    _S = ctypes.c_char_p
+    L.pllgpu_resume.argtypes = [_VP, _D]
+    L.pllgpu_write_snapshot.argtypes = [_VP, _I, _S]
+    L.pllgpu_write_snapshot_ex.argtypes = [_VP, _I, _I, _S, _I]
+    L.pllgpu_write_restart.argtypes = [_VP, _I, _I, _D, _D, _D, _D, _S]
+    L.pllgpu_read_restart.argtypes = [_VP, _S, ctypes.POINTER(_I), ctypes.POINTER(_I), _PD, _PD]
+    L.pllgpu_conc_average.argtypes = [_VP, _D, _S]
+    L.pllgpu_find_wmax.argtypes = [_VP, _D, _S, _PD]
+    L.pllgpu_find_max.argtypes = [_VP, _S, _PD, ctypes.POINTER(_I)]
     _lib = L
     return L
 
@@ -125,4 +134,7 @@ EXPORTED_SYMBOLS = [
     "pllgpu_stream", "pllgpu_profile_steps", "pllgpu_dct2d_batch_noalloc",
     "pllgpu_set_timestep", "pllgpu_set_tval", "pllgpu_acoef", "pllgpu_weno_batch",
     "pllgpu_tridiag_1rhs_batch", "pllgpu_idct2d_batch", "pllgpu_diagnostics",
+    "pllgpu_resume", "pllgpu_write_snapshot", "pllgpu_write_snapshot_ex",
+    "pllgpu_write_restart", "pllgpu_read_restart", "pllgpu_conc_average",
+    "pllgpu_find_wmax", "pllgpu_find_max",
 ]

@@ -70,6 +70,7 @@ struct pllgpu_ctx {
     double* work = nullptr;     // slope-parameter scratch
     double* diag = nullptr;     // per-plane diagnostics + results
     int cur = 0;                // buffer index holding the "old" role
+    bool resync_c = false;      // after a restart: copy c's buffers once (resume)
     bool rotated = false;       // fast steps ran: "new" roles are stale and
                                 // logically equal to "old" (see materialize)
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};

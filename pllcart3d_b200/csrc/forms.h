@@ -9,6 +9,8 @@ void form_enqueue_step_f64(pllgpu_ctx* c);
 void form_enqueue_step_f32(pllgpu_ctx* c);
 int form_start_f64(pllgpu_ctx* c);
 int form_start_f32(pllgpu_ctx* c);
+int form_resume_f64(pllgpu_ctx* c);
+int form_resume_f32(pllgpu_ctx* c);
 int form_routine_f64(pllgpu_ctx* c, int routine, const double* in, double* out);
 int form_routine_f32(pllgpu_ctx* c, int routine, const double* in, double* out);
 int form_materialize_f64(pllgpu_ctx* c);
@@ -19,5 +21,10 @@ void form_diag_f64(pllgpu_ctx* c);
 void form_diag_f32(pllgpu_ctx* c);
 bool form_alloc_f64(pllgpu_ctx* c);
 bool form_alloc_f32(pllgpu_ctx* c);
+
+// runtime.cu: the field of id f in the form's storage type, with the
+// reference's new == old view after fast steps (a write materialises "new")
+void* field_ptr(pllgpu_ctx* c, int f, bool for_write);
+int materialize(pllgpu_ctx* c);
 
 }  // namespace pll

@@ -284,6 +284,16 @@ void enqueue_substep(pllgpu_ctx* ctx, int rk)
     launch_phi_ghosts<real>(ctx);
     launch_project<real>(ctx, alpha, 1, 1, 1);
     ctx->cur ^= 1;  // update_old_*: roles swap
+    if (ctx->resync_c) {
+        // After a restart the reference's c->new holds values its routines
+        // never write (intermediate() restores c->old only, pllcart3d.c:3209)
+        // and update_old_conc copies them into c->old after this substep;
+        // one full copy makes the two buffers agree there from now on.
+        if (cudaMemcpyAsync(q_new<real>(ctx, VC), q_old<real>(ctx, VC), sizeof(real) * (size_t)ctx->nelem,
+                            cudaMemcpyDeviceToDevice, ctx->st) != cudaSuccess)
+            fail(ctx, PLLGPU_ECUDA);
+        ctx->resync_c = false;
+    }
 }
 
 __global__ void k_tval(double* scal, double a0, double a1, double a2)
@@ -342,16 +352,22 @@ real* field_ptr_raw(pllgpu_ctx* ctx, int f)
 
 // ---- start-up, routines ---------------------------------------------------------
 
+// start-up of pllcart3d.c:75-142.  fresh: after an initial condition
+// (ghosts, then new -> old); otherwise after intermediate() restored the
+// state (L111), where only the viscosity start-up follows.
 template <typename real>
-int start_t(pllgpu_ctx* ctx)
+int start_t(pllgpu_ctx* ctx, bool fresh = true)
 {
     const size_t bytes = sizeof(real) * (size_t)ctx->nelem;
-    // update_ghost_points (L81) on the initial velocities; phi is zero
-    launch_project<real>(ctx, 0.0, 0, 1, 0);
-    // update_old_conc / update_old_velo (L82-83): both buffers equal
-    for (int v = 0; v < 4; ++v) {
-        CK(cudaMemcpyAsync(q_old<real>(ctx, v), q_new<real>(ctx, v), bytes, cudaMemcpyDeviceToDevice, ctx->st));
-        CK(cudaMemcpyAsync(h_nm1<real>(ctx, v), h_n<real>(ctx, v), bytes, cudaMemcpyDeviceToDevice, ctx->st));
+    if (fresh) {
+        // update_ghost_points (L81) on the initial velocities; phi is zero
+        launch_project<real>(ctx, 0.0, 0, 1, 0);
+        // update_old_conc / update_old_velo (L82-83): both buffers equal
+        for (int v = 0; v < 4; ++v) {
+            CK(cudaMemcpyAsync(q_old<real>(ctx, v), q_new<real>(ctx, v), bytes, cudaMemcpyDeviceToDevice,
+                               ctx->st));
+            CK(cudaMemcpyAsync(h_nm1<real>(ctx, v), h_n<real>(ctx, v), bytes, cudaMemcpyDeviceToDevice, ctx->st));
+        }
     }
     if (ctx->P.nmvp) {
         const double PI = 4.0 * std::atan(1.0);
@@ -653,6 +669,7 @@ bool alloc_state(pllgpu_ctx* c)
     namespace pll {                                                                          \
     void form_enqueue_step_##SUFFIX(pllgpu_ctx* c) { enqueue_step<REAL>(c); }                \
     int form_start_##SUFFIX(pllgpu_ctx* c) { return start_t<REAL>(c); }                      \
+    int form_resume_##SUFFIX(pllgpu_ctx* c) { return start_t<REAL>(c, false); }              \
     int form_routine_##SUFFIX(pllgpu_ctx* c, int r, const double* in, double* out)           \
     {                                                                                        \
         return routine_t<REAL>(c, r, in, out);                                               \

@@ -93,7 +93,30 @@ int new_to_old(int f)
     }
 }
 
-int materialize_t_any(pllgpu_ctx* ctx)
+template <int VAR>
+__global__ void k_acoef(Geo G, Rng R, Consts K, MuPtrs<double> mu, double* __restrict__ abc, long nelem)
+{
+    const int k = R.ks + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = R.js + blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = R.is + blockIdx.z;
+    if (k > R.ke || j > R.je) return;
+    const long id = (long)i * G.sx + (long)j * G.sy + k;
+    double a, b, c;
+    acoef<VAR, 0, double>(K, G, mu.cell, mu.xy, mu.xz, mu.yz, id, a, b, c);
+    abc[id] = a; abc[nelem + id] = b; abc[2 * nelem + id] = c;
+    acoef<VAR, 1, double>(K, G, mu.cell, mu.xy, mu.xz, mu.yz, id, a, b, c);
+    abc[3 * nelem + id] = a; abc[4 * nelem + id] = b; abc[5 * nelem + id] = c;
+    acoef<VAR, 2, double>(K, G, mu.cell, mu.xy, mu.xz, mu.yz, id, a, b, c);
+    abc[6 * nelem + id] = a; abc[7 * nelem + id] = b; abc[8 * nelem + id] = c;
+}
+
+
+}  // namespace
+}  // namespace pll
+
+namespace pll {
+
+static int materialize_t_any(pllgpu_ctx* ctx)
 {
     return ctx->mixed ? form_materialize_f32(ctx) : form_materialize_f64(ctx);
 }
@@ -118,25 +141,6 @@ void* field_ptr(pllgpu_ctx* ctx, int f, bool for_write)
     return ctx->mixed ? form_field_ptr_f32(ctx, f) : form_field_ptr_f64(ctx, f);
 }
 
-template <int VAR>
-__global__ void k_acoef(Geo G, Rng R, Consts K, MuPtrs<double> mu, double* __restrict__ abc, long nelem)
-{
-    const int k = R.ks + blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = R.js + blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = R.is + blockIdx.z;
-    if (k > R.ke || j > R.je) return;
-    const long id = (long)i * G.sx + (long)j * G.sy + k;
-    double a, b, c;
-    acoef<VAR, 0, double>(K, G, mu.cell, mu.xy, mu.xz, mu.yz, id, a, b, c);
-    abc[id] = a; abc[nelem + id] = b; abc[2 * nelem + id] = c;
-    acoef<VAR, 1, double>(K, G, mu.cell, mu.xy, mu.xz, mu.yz, id, a, b, c);
-    abc[3 * nelem + id] = a; abc[4 * nelem + id] = b; abc[5 * nelem + id] = c;
-    acoef<VAR, 2, double>(K, G, mu.cell, mu.xy, mu.xz, mu.yz, id, a, b, c);
-    abc[6 * nelem + id] = a; abc[7 * nelem + id] = b; abc[8 * nelem + id] = c;
-}
-
-
-}  // namespace
 }  // namespace pll
 
 // ---------------------------------------------------------------------------
@@ -349,10 +353,32 @@ int pllgpu_start(pllgpu_ctx* ctx)
     return read_status(ctx);
 }
 
+int pllgpu_resume(pllgpu_ctx* ctx, double tval)
+{
+    if (!ctx) return PLLGPU_EINVAL;
+    CK(cudaSetDevice(ctx->dev));
+    if (int e = materialize(ctx)) return e;
+    int e = ctx->mixed ? form_resume_f32(ctx) : form_resume_f64(ctx);
+    if (e) return e;
+    ctx->resync_c = true;
+    if (int e2 = check_launch(ctx)) return e2;
+    CK(cudaStreamSynchronize(ctx->st));
+    set_scalar(ctx, S_TVAL, tval);
+    return read_status(ctx);
+}
+
 int pllgpu_steps(pllgpu_ctx* ctx, int nsteps)
 {
     if (!ctx || nsteps < 0) return PLLGPU_EINVAL;
     CK(cudaSetDevice(ctx->dev));
+    if (ctx->resync_c && nsteps > 0) {
+        // first step after a restart on the stream (it carries one extra copy)
+        ctx->counting = 0;
+        enqueue_step_any(ctx);
+        if (int e = check_launch(ctx)) return e;
+        ctx->rotated = true;
+        --nsteps;
+    }
     if (ctx->P.use_graph) {
         if (!ctx->graphs_ready) {
             if (int e = build_graphs(ctx)) return e;

@@ -132,6 +132,52 @@ class Solver:
         self._check(self._L.pllgpu_diagnostics(self._h, out), "diagnostics")
         return {"mass": out[0], "div_max": out[1], "div_l2": out[2], "mixing_length": out[3]}
 
+    # ---- the reference's output files (write_to_file, midfield, ...) --------
+    def write_snapshot(self, fileno: int, directory: str = ".", subsample=None) -> None:
+        """write_to_file, pllcart3d.c:3047: caf%04dR000.bin in `directory`;
+        subsample None follows the reference's 2e7-cell rule."""
+        sub = -1 if subsample is None else int(bool(subsample))
+        self._check(self._L.pllgpu_write_snapshot_ex(self._h, int(fileno), 0, directory.encode(), sub),
+                    "write_snapshot")
+
+    def write_restart(self, tstep: int, fileno: int, tval: float, outtime: float, outmid: float,
+                      cavgtime: float, directory: str = ".") -> None:
+        """midfield, pllcart3d.c:3121: middata + midfield000.bin."""
+        self._check(self._L.pllgpu_write_restart(self._h, int(tstep), int(fileno), float(tval),
+                                                 float(outtime), float(outmid), float(cavgtime),
+                                                 directory.encode()), "write_restart")
+
+    def read_restart(self, directory: str = ".") -> dict:
+        """intermediate, pllcart3d.c:3181, then the restart start-up."""
+        ts, fn = ctypes.c_int(), ctypes.c_int()
+        tv, ot = ctypes.c_double(), ctypes.c_double()
+        self._check(self._L.pllgpu_read_restart(self._h, directory.encode(), ctypes.byref(ts),
+                                                ctypes.byref(fn), ctypes.byref(tv), ctypes.byref(ot)),
+                    "read_restart")
+        self._check(self._L.pllgpu_resume(self._h, tv.value), "resume")
+        return {"tstep": ts.value, "fileno": fn.value, "tval": tv.value, "outtime": ot.value}
+
+    def conc_average(self, tval: float, directory: str = ".") -> None:
+        """conc_average, pllcart3d.c:3635: appends cavgy/cavgz/cavgyz.bin."""
+        self._check(self._L.pllgpu_conc_average(self._h, float(tval), directory.encode()), "conc_average")
+
+    def find_wmax(self, tval: float, directory=None) -> float:
+        """find_wmax, pllcart3d.c:3606 (appends wmax.bin when a directory is given)."""
+        out = ctypes.c_double()
+        d = directory.encode() if directory is not None else None
+        self._check(self._L.pllgpu_find_wmax(self._h, float(tval), d, ctypes.byref(out)), "find_wmax")
+        return out.value
+
+    def find_max(self, directory=None) -> dict:
+        """find_max, pllcart3d.c:3539: max |u|,|v|,|w|,|c| (signed value at
+        the last index attaining it) and where; appends to Outscreen when a
+        directory is given.  A NaN in c raises PllGpuError (ENAN)."""
+        val = (ctypes.c_double * 4)()
+        loc = (ctypes.c_int * 12)()
+        d = directory.encode() if directory is not None else None
+        self._check(self._L.pllgpu_find_max(self._h, d, val, loc), "find_max")
+        return {q: (val[n], tuple(loc[3 * n:3 * n + 3])) for n, q in enumerate("uvwc")}
+
     def status(self) -> int:
         return self._L.pllgpu_status(self._h)
 
