@@ -247,6 +247,13 @@ int pllgpu_find_wmax(pllgpu_ctx *ctx, double tval, const char *dir,
 int pllgpu_find_max(pllgpu_ctx *ctx, const char *dir, double *maxval,
                     int *maxloc);
 
+/* shift_conc (pllcart3d.c:3231, spline L3280): the spanwise wave
+ * perturbation of c_old, each x line re-sampled at x - meshdx(z) by a natural
+ * cubic spline; meshdx = ampli cos(2 pi z / lamb) (+ the sub-harmonic term
+ * when subharm = 1).  The reference's Ampli, Lamb and Subharm of
+ * param.input; it calls this once, at tval >= 2 with Wavpert = 1 (L247). */
+int pllgpu_shift_conc(pllgpu_ctx *ctx, double ampli, double lamb, int subharm);
+
 #define PLLGPU_DCT_NOALLOC_MAX_DOUBLES (1L << 21)
 int pllgpu_dct2d_batch_noalloc(int kind, int n0, int n1, int howmany,
                                const double *d_in, double *d_out,

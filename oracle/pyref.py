@@ -136,6 +136,11 @@ class RefRun:
     def find_max(self, directory: str) -> None:
         assert self.lib.pllref_find_max(directory.encode()) == 0
 
+    def shift_conc(self, ampli: float, lamb: float, subharm: int) -> None:
+        f = self.lib.pllref_shift_conc
+        f.argtypes = [_D, _D, _I]
+        f(ampli, lamb, subharm)
+
     @property
     def dt(self) -> float:
         return self.lib.pllref_last_dt()

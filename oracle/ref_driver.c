@@ -85,6 +85,7 @@ void intermediate(int *, int *, double *, double *, Grid *, Conc *, Velo *, Velo
 void conc_average(Grid *, double ***, double);
 void find_wmax(double, Grid *, Velo *);
 void find_max(Grid *, Velo *, Velo *, Velo *, Conc *);
+void shift_conc(Grid *, Conc *);
 
 static Grid *g_grid;
 static Velo *g_u, *g_v, *g_w;
@@ -541,4 +542,13 @@ int pllref_find_max(const char *dir)
     if (in_dir(dir, here)) return -1;
     find_max(g_grid, g_u, g_v, g_w, g_c);
     return chdir(here);
+}
+
+/* shift_conc (pllcart3d.c:3231) with the given wave parameters */
+void pllref_shift_conc(double ampli, double lamb, int subharm)
+{
+    Ampli = ampli;
+    Lamb = lamb;
+    Subharm = subharm;
+    shift_conc(g_grid, g_c);
 }

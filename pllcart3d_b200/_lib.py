@@ -120,6 +120,7 @@ def lib():
     L.pllgpu_conc_average.argtypes = [_VP, _D, _S]
     L.pllgpu_find_wmax.argtypes = [_VP, _D, _S, _PD]
     L.pllgpu_find_max.argtypes = [_VP, _S, _PD, ctypes.POINTER(_I)]
+    L.pllgpu_shift_conc.argtypes = [_VP, _D, _D, _I]
     _lib = L
     return L
 
@@ -136,5 +137,5 @@ EXPORTED_SYMBOLS = [
     "pllgpu_tridiag_1rhs_batch", "pllgpu_idct2d_batch", "pllgpu_diagnostics",
     "pllgpu_resume", "pllgpu_write_snapshot", "pllgpu_write_snapshot_ex",
     "pllgpu_write_restart", "pllgpu_read_restart", "pllgpu_conc_average",
-    "pllgpu_find_wmax", "pllgpu_find_max",
+    "pllgpu_find_wmax", "pllgpu_find_max", "pllgpu_shift_conc",
 ]

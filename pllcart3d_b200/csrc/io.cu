@@ -471,6 +471,7 @@ int pllgpu_read_restart(pllgpu_ctx* ctx, const char* dir, int* tstep, int* filen
                     fscanf(fp, "%lf\n", outtime);
     fclose(fp);
     if (got != 4) return fail(ctx, PLLGPU_EINVAL);
+    if (int e = materialize(ctx)) return e;
     fp = fopen(in_dir(dir, "midfield000.bin").c_str(), "rb");
     if (!fp) return fail(ctx, PLLGPU_EINVAL);
     const int e = ctx->mixed ? read_mid_t<float>(ctx, fp) : read_mid_t<double>(ctx, fp);

@@ -178,6 +178,15 @@ class Solver:
         self._check(self._L.pllgpu_find_max(self._h, d, val, loc), "find_max")
         return {q: (val[n], tuple(loc[3 * n:3 * n + 3])) for n, q in enumerate("uvwc")}
 
+    def shift_conc(self, ampli=None, lamb=None, subharm=None) -> None:
+        """shift_conc, pllcart3d.c:3231: the spanwise wave perturbation of
+        c_old (defaults: the run's Ampli, Lamb, Subharm)."""
+        p = self.params
+        a = p.Ampli if ampli is None else ampli
+        lm = p.Lamb if lamb is None else lamb
+        sh = p.Subharm if subharm is None else subharm
+        self._check(self._L.pllgpu_shift_conc(self._h, float(a), float(lm), int(sh)), "shift_conc")
+
     def status(self) -> int:
         return self._L.pllgpu_status(self._h)
 
