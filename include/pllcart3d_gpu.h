@@ -254,6 +254,33 @@ int pllgpu_find_max(pllgpu_ctx *ctx, const char *dir, double *maxval,
  * param.input; it calls this once, at tval >= 2 with Wavpert = 1 (L247). */
 int pllgpu_shift_conc(pllgpu_ctx *ctx, double ampli, double lamb, int subharm);
 
+/* ---- launch-shape autotuner ----------------------------------------------
+ * Times every launch-shape variant of the explicit operators (4) and the x/y
+ * line solves (3) on `trial_steps` steps each (plus one warm-up step) and
+ * keeps the fastest.  All variants compute bit-identical results, so the
+ * trial steps are steps of the run; *steps_done reports how many. */
+int pllgpu_autotune(pllgpu_ctx *ctx, int trial_steps, int *steps_done);
+int pllgpu_tuning(pllgpu_ctx *ctx, int *explicit_variant, int *line_variant);
+int pllgpu_set_tuning(pllgpu_ctx *ctx, int explicit_variant, int line_variant);
+
+/* ---- ensembles ------------------------------------------------------------
+ * n independent runs (each its own grid and parameters, params[i]) on one
+ * device, advanced together: one CUDA graph per step holds every member's
+ * step as a parallel branch.  Members are ordinary contexts
+ * (pllgpu_ensemble_member): set their fields and read them with the calls
+ * above.  Every member computes exactly what it computes alone. */
+typedef struct pllgpu_ensemble pllgpu_ensemble;
+pllgpu_ensemble *pllgpu_ensemble_create(int n, const pllgpu_params *params,
+                                        int device);
+void pllgpu_ensemble_destroy(pllgpu_ensemble *ens);
+int pllgpu_ensemble_size(const pllgpu_ensemble *ens);
+pllgpu_ctx *pllgpu_ensemble_member(pllgpu_ensemble *ens, int i);
+int pllgpu_ensemble_start(pllgpu_ensemble *ens);
+int pllgpu_ensemble_steps(pllgpu_ensemble *ens, int nsteps);
+int pllgpu_ensemble_autotune(pllgpu_ensemble *ens, int trial_steps,
+                             int *steps_done);
+int pllgpu_ensemble_launches_per_step(const pllgpu_ensemble *ens);
+
 #define PLLGPU_DCT_NOALLOC_MAX_DOUBLES (1L << 21)
 int pllgpu_dct2d_batch_noalloc(int kind, int n0, int n1, int howmany,
                                const double *d_in, double *d_out,

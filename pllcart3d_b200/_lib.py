@@ -121,6 +121,20 @@ def lib():
     L.pllgpu_find_wmax.argtypes = [_VP, _D, _S, _PD]
     L.pllgpu_find_max.argtypes = [_VP, _S, _PD, ctypes.POINTER(_I)]
     L.pllgpu_shift_conc.argtypes = [_VP, _D, _D, _I]
+    _PI = ctypes.POINTER(_I)
+    L.pllgpu_autotune.argtypes = [_VP, _I, _PI]
+    L.pllgpu_tuning.argtypes = [_VP, _PI, _PI]
+    L.pllgpu_set_tuning.argtypes = [_VP, _I, _I]
+    L.pllgpu_ensemble_create.restype = _VP
+    L.pllgpu_ensemble_create.argtypes = [_I, ctypes.POINTER(Params), _I]
+    L.pllgpu_ensemble_destroy.argtypes = [_VP]
+    L.pllgpu_ensemble_size.argtypes = [_VP]
+    L.pllgpu_ensemble_member.restype = _VP
+    L.pllgpu_ensemble_member.argtypes = [_VP, _I]
+    L.pllgpu_ensemble_start.argtypes = [_VP]
+    L.pllgpu_ensemble_steps.argtypes = [_VP, _I]
+    L.pllgpu_ensemble_autotune.argtypes = [_VP, _I, _PI]
+    L.pllgpu_ensemble_launches_per_step.argtypes = [_VP]
     _lib = L
     return L
 
@@ -138,4 +152,8 @@ EXPORTED_SYMBOLS = [
     "pllgpu_resume", "pllgpu_write_snapshot", "pllgpu_write_snapshot_ex",
     "pllgpu_write_restart", "pllgpu_read_restart", "pllgpu_conc_average",
     "pllgpu_find_wmax", "pllgpu_find_max", "pllgpu_shift_conc",
+    "pllgpu_autotune", "pllgpu_tuning", "pllgpu_set_tuning",
+    "pllgpu_ensemble_create", "pllgpu_ensemble_destroy", "pllgpu_ensemble_size",
+    "pllgpu_ensemble_member", "pllgpu_ensemble_start", "pllgpu_ensemble_steps",
+    "pllgpu_ensemble_autotune", "pllgpu_ensemble_launches_per_step",
 ]

@@ -35,7 +35,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17",
 CU_SOURCES = {"runtime.cu": "--fmad=false", "form_f64.cu": "--fmad=false",
               "form_f32.cu": "--fmad=true", "primitives.cu": "--fmad=false",
               "noalloc.cu": "--fmad=false", "io.cu": "--fmad=false",
-              "wave.cu": "--fmad=false"}
+              "wave.cu": "--fmad=false", "ensemble.cu": "--fmad=false"}
 HEADERS = ["common.cuh", "step_kernels.cuh", "aux_kernels.cuh", "dct_kernels.cuh", "host_util.h",
            "ctx.cuh", "host_common.cuh", "orchestrate.cuh", "forms.h", "umma_dct.cuh"]
 

@@ -89,4 +89,20 @@ struct MuPtrs {
     const real* yz;
 };
 
+// launch-shape variants the autotuner chooses among; every variant computes
+// each cell (explicit operators) or line (line solves) with the same
+// arithmetic, so the choice changes timing only, never a bit of the result
+constexpr int NTUNE_EXP = 4, NTUNE_LINE = 3;
+inline void tune_exp_block(int v, int& bx, int& by)
+{
+    static const int t[NTUNE_EXP][2] = {{32, 4}, {64, 2}, {128, 1}, {32, 2}};
+    bx = t[v][0];
+    by = t[v][1];
+}
+inline int tune_line_block(int v)
+{
+    static const int t[NTUNE_LINE] = {32, 64, 128};
+    return t[v];
+}
+
 }  // namespace pll

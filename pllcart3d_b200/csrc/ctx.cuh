@@ -71,6 +71,8 @@ struct pllgpu_ctx {
     double* diag = nullptr;     // per-plane diagnostics + results
     int cur = 0;                // buffer index holding the "old" role
     bool resync_c = false;      // after a restart: copy c's buffers once (resume)
+    int tune_exp = 0;           // launch-shape variants (autotuner): explicit-
+    int tune_line = 1;          // operator block, x/y line-solve block
     bool rotated = false;       // fast steps ran: "new" roles are stale and
                                 // logically equal to "old" (see materialize)
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};

@@ -25,6 +25,8 @@ bool form_alloc_f32(pllgpu_ctx* c);
 // runtime.cu: the field of id f in the form's storage type, with the
 // reference's new == old view after fast steps (a write materialises "new")
 void* field_ptr(pllgpu_ctx* c, int f, bool for_write);
+// one full step of either form on the context's stream (runtime.cu)
+void enqueue_step_any(pllgpu_ctx* c);
 int materialize(pllgpu_ctx* c);
 
 }  // namespace pll

@@ -45,7 +45,9 @@ void launch_explicit(pllgpu_ctx* ctx, const real* un, const real* vn, const real
     A.g = g;
     A.r = r;
     A.alpha = g + r;
-    dim3 blk(32, 4);
+    int bx, by;
+    tune_exp_block(ctx->tune_exp, bx, by);
+    const dim3 blk(bx, by);
     k_explicit<VAR, real><<<box_grid(nk(R), nj(R), ni(R), blk), blk, 0, ctx->st>>>(ctx->G, R, ctx->K, A);
     mark(ctx, lab[VAR]);
 }
@@ -71,13 +73,14 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
     X.g = g;
     X.r = r;
     X.alpha = alpha;
-    k_line_pf<VAR, 1, real><<<dim3((nk(R) + 63) / 64, ni(R)), 64, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
+    const int lb = tune_line_block(ctx->tune_line);
+    k_line_pf<VAR, 1, real><<<dim3((nk(R) + lb - 1) / lb, ni(R)), lb, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
     mark(ctx, ly[VAR]);
     constexpr size_t smem = adi_z_smem_bytes<VAR, real>();
     k_adi_z_tiled<VAR, real><<<dim3((nj(R) + 127) / 128, ni(R)), 128, smem, ctx->st>>>(
         ctx->G, R, ctx->K, X.mu, B.S, B.cc, ctx->scal, alpha);
     mark(ctx, lz[VAR]);
-    k_line_pf<VAR, 0, real><<<dim3((nk(R) + 63) / 64, nj(R)), 64, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
+    k_line_pf<VAR, 0, real><<<dim3((nk(R) + lb - 1) / lb, nj(R)), lb, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
     mark(ctx, lx[VAR]);
 }
 

@@ -40,13 +40,14 @@
 using namespace pll;
 
 namespace pll {
-namespace {
 
 void enqueue_step_any(pllgpu_ctx* ctx)
 {
     if (ctx->mixed) form_enqueue_step_f32(ctx);
     else form_enqueue_step_f64(ctx);
 }
+
+namespace {
 
 int build_graphs(pllgpu_ctx* ctx)
 {
@@ -398,6 +399,83 @@ int pllgpu_steps(pllgpu_ctx* ctx, int nsteps)
     if (nsteps > 0) ctx->rotated = true;
     CK(cudaStreamSynchronize(ctx->st));
     return read_status(ctx);
+}
+
+int pllgpu_autotune(pllgpu_ctx* ctx, int trial_steps, int* steps_done)
+{
+    if (!ctx || trial_steps < 1) return PLLGPU_EINVAL;
+    CK(cudaSetDevice(ctx->dev));
+    if (int e = materialize(ctx)) return e;
+    // Every variant computes bit-identical results, so the trials are steps
+    // of the run itself: nothing is saved or restored, and the state after
+    // tuning equals the state of the same number of untuned steps.
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    int best_e = ctx->tune_exp, best_l = ctx->tune_line, done = 0;
+    float best = 1e30f;
+    if (ctx->resync_c) {   // the restart copy runs on the first step
+        enqueue_step_any(ctx);
+        ++done;
+    }
+    for (int ve = 0; ve < NTUNE_EXP; ++ve)
+        for (int vl = 0; vl < NTUNE_LINE; ++vl) {
+            ctx->tune_exp = ve;
+            ctx->tune_line = vl;
+            enqueue_step_any(ctx);   // warm-up of this variant
+            CK(cudaEventRecord(e0, ctx->st));
+            for (int s = 0; s < trial_steps; ++s) enqueue_step_any(ctx);
+            CK(cudaEventRecord(e1, ctx->st));
+            if (int e = check_launch(ctx)) return e;
+            CK(cudaEventSynchronize(e1));
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            done += trial_steps + 1;
+            if (ms < best) {
+                best = ms;
+                best_e = ve;
+                best_l = vl;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->tune_exp = best_e;
+    ctx->tune_line = best_l;
+    // graphs captured with the old shapes are rebuilt on the next steps call
+    for (int t = 0; t < 2; ++t)
+        if (ctx->gexec[t]) {
+            cudaGraphExecDestroy(ctx->gexec[t]);
+            ctx->gexec[t] = nullptr;
+        }
+    ctx->graphs_ready = false;
+    ctx->rotated = true;
+    if (steps_done) *steps_done = done;
+    CK(cudaStreamSynchronize(ctx->st));
+    return read_status(ctx);
+}
+
+int pllgpu_tuning(pllgpu_ctx* ctx, int* explicit_variant, int* line_variant)
+{
+    if (!ctx) return PLLGPU_EINVAL;
+    if (explicit_variant) *explicit_variant = ctx->tune_exp;
+    if (line_variant) *line_variant = ctx->tune_line;
+    return PLLGPU_OK;
+}
+
+int pllgpu_set_tuning(pllgpu_ctx* ctx, int explicit_variant, int line_variant)
+{
+    if (!ctx || explicit_variant < 0 || explicit_variant >= NTUNE_EXP || line_variant < 0 ||
+        line_variant >= NTUNE_LINE)
+        return PLLGPU_EINVAL;
+    ctx->tune_exp = explicit_variant;
+    ctx->tune_line = line_variant;
+    for (int t = 0; t < 2; ++t)
+        if (ctx->gexec[t]) {
+            cudaGraphExecDestroy(ctx->gexec[t]);
+            ctx->gexec[t] = nullptr;
+        }
+    ctx->graphs_ready = false;
+    return PLLGPU_OK;
 }
 
 int pllgpu_run_host(pllgpu_ctx* ctx, int nsteps, const double* c0, const double* u0, const double* v0,

@@ -38,9 +38,29 @@ class Solver:
 
     def __init__(self, params: Params, device: int = 0, exact_dct: bool = False,
                  use_graph: bool = True, precision: str = "fp64", dct_kernel: str = "auto"):
-        params.validate()
+        p = self.c_params(params, exact_dct, use_graph, precision, dct_kernel)
         self.params = params
-        L = _lib.lib()
+        self.precision = precision
+        self._L = _lib.lib()
+        self._owned = True
+        self._h = self._L.pllgpu_create(ctypes.byref(p), int(device))
+        if not self._h:
+            raise _lib.PllGpuError(2, "pllgpu_create")
+        self.shape = params.shape
+
+    @classmethod
+    def view(cls, handle, params: Params, precision: str) -> "Solver":
+        """A Solver over a context owned elsewhere (an ensemble member)."""
+        s = cls.__new__(cls)
+        s.params, s.precision, s._L, s._owned, s._h = params, precision, _lib.lib(), False, handle
+        s.shape = params.shape
+        return s
+
+    @staticmethod
+    def c_params(params: Params, exact_dct: bool = False, use_graph: bool = True,
+                 precision: str = "fp64", dct_kernel: str = "auto"):
+        """The pllgpu_params struct of a run."""
+        params.validate()
         p = _lib.Params()
         p.nx, p.ny, p.nz = params.nx, params.ny, params.nz
         p.nmvp = params.Nmvp
@@ -50,20 +70,16 @@ class Solver:
         p.Fx, p.Fy, p.CFLmax = params.Fx, params.Fy, params.CFLmax
         p.Timestep, p.Mum, p.Lambda = params.Timestep, params.Mum, params.Lambda
         p.precision = PRECISIONS[precision]
-        self.precision = precision
         p.exact_dct = int(bool(exact_dct))
         p.use_graph = int(bool(use_graph))
         p.dct_kernel = {"auto": 0, "mma_sync": 1}[dct_kernel]
-        self._L = L
-        self._h = L.pllgpu_create(ctypes.byref(p), int(device))
-        if not self._h:
-            raise _lib.PllGpuError(2, "pllgpu_create")
-        self.shape = params.shape
+        return p
 
     # ---- lifetime ---------------------------------------------------------
     def close(self) -> None:
         if getattr(self, "_h", None):
-            self._L.pllgpu_destroy(self._h)
+            if getattr(self, "_owned", True):
+                self._L.pllgpu_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -186,6 +202,22 @@ class Solver:
         lm = p.Lamb if lamb is None else lamb
         sh = p.Subharm if subharm is None else subharm
         self._check(self._L.pllgpu_shift_conc(self._h, float(a), float(lm), int(sh)), "shift_conc")
+
+    def autotune(self, trial_steps: int = 2) -> int:
+        """pllgpu_autotune: picks the fastest launch shapes on steps of this
+        run (bit-identical variants); returns the steps it advanced."""
+        done = ctypes.c_int()
+        self._check(self._L.pllgpu_autotune(self._h, int(trial_steps), ctypes.byref(done)), "autotune")
+        return done.value
+
+    def tuning(self) -> tuple:
+        e, l = ctypes.c_int(), ctypes.c_int()
+        self._check(self._L.pllgpu_tuning(self._h, ctypes.byref(e), ctypes.byref(l)), "tuning")
+        return e.value, l.value
+
+    def set_tuning(self, explicit_variant: int, line_variant: int) -> None:
+        self._check(self._L.pllgpu_set_tuning(self._h, int(explicit_variant), int(line_variant)),
+                    "set_tuning")
 
     def status(self) -> int:
         return self._L.pllgpu_status(self._h)
