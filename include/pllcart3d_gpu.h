@@ -281,6 +281,20 @@ int pllgpu_ensemble_autotune(pllgpu_ensemble *ens, int trial_steps,
                              int *steps_done);
 int pllgpu_ensemble_launches_per_step(const pllgpu_ensemble *ens);
 
+/* the whole state of src (fields of both buffer roles, viscosity,
+ * pressure gradient, phi, device scalars) into dst, device to device; both
+ * of the same grid and form.  No reference counterpart. */
+int pllgpu_copy_state(pllgpu_ctx *dst, pllgpu_ctx *src);
+
+/* cell-centred (u, v, w, c) float32 of every interior cell, i-j-k order
+ * ([nx][ny][nz][4]), into / out of a caller's device buffer (16-byte
+ * aligned): the state exchange of a learned model.  unpack writes c's
+ * interior (with its y/z Neumann ghosts) and the interior faces of u, v, w
+ * (mean of the two adjacent centres) into the *_new fields; boundary faces
+ * keep their values.  No reference counterpart. */
+int pllgpu_pack_cells(pllgpu_ctx *ctx, float *d_cells);
+int pllgpu_unpack_cells(pllgpu_ctx *ctx, const float *d_cells);
+
 #define PLLGPU_DCT_NOALLOC_MAX_DOUBLES (1L << 21)
 int pllgpu_dct2d_batch_noalloc(int kind, int n0, int n1, int howmany,
                                const double *d_in, double *d_out,

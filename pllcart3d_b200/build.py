@@ -4,6 +4,8 @@
   the FP64 step is compiled with ``--fmad=false`` so that no multiply-add is
   contracted (the reference's own arithmetic has none), the precision form's
   FP32 kernels with contraction;
+* ``libpllnn.so``            - the learned surrogate's BF16 tensor-core kernels
+  (convolution forward / backward, pooling, upsampling, Adam);
 * ``libpllcart3d_dropin.so`` - the reference-signature drop-in layer (plain C,
   compiled with gcc because the reference's structures name a member ``new``).
 
@@ -22,6 +24,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INC = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libpllgpu.so")
+NNLIB = os.path.join(HERE, "libpllnn.so")
 DROPIN = os.path.join(HERE, "libpllcart3d_dropin.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -72,6 +75,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
         subprocess.run(cmd, check=True)
         for o in objs:
             os.remove(o)
+    nsrc = os.path.join(CSRC, "nn.cu")
+    if os.path.exists(nsrc) and (force or _stale(NNLIB, [nsrc, __file__])):
+        cmd = [_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas",
+               "-warn-spills", "-shared", "-cudart", "static", nsrc, "-o", NNLIB]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
     dsrc = os.path.join(CSRC, "dropin.c")
     if os.path.exists(dsrc) and (force or _stale(DROPIN, [dsrc, LIB, os.path.join(INC, "pllcart3d_gpu.h")])):
         cmd = ["gcc", "-O2", "-fPIC", "-shared", "-std=gnu99", "-Wall", "-I", INC,

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -56,6 +57,44 @@ __global__ void k_pack_caf(Geo G, const real* __restrict__ u, const real* __rest
     out[4 * t + 1] = (float)vval;
     out[4 * t + 2] = (float)wval;
     out[4 * t + 3] = (float)(double)c[id];
+}
+
+// the inverse for a learned model's prediction: cell-centred (u, v, w, c)
+// back into c's interior (and its y/z Neumann ghosts, as the x sweep of
+// concentration fills them) and the interior faces of u, v, w (the mean of
+// the two adjacent cell centres); inlet, outlet and wall faces keep their
+// values
+template <typename real>
+__global__ void k_unpack_cells(Geo G, Rng R, const float4* __restrict__ cells, real* __restrict__ c,
+                               real* __restrict__ u, real* __restrict__ v, real* __restrict__ w)
+{
+    const int k = R.ks + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = R.js + blockIdx.y;
+    const int i = R.is + blockIdx.z;
+    if (k > R.ke) return;
+    const int nj = R.je - R.js + 1, nk = R.ke - R.ks + 1;
+    auto cell = [&](int ii, int jj, int kk) {
+        return cells[((long)(ii - R.is) * nj + (jj - R.js)) * nk + (kk - R.ks)];
+    };
+    const long id = (long)i * G.sx + (long)j * G.sy + k;
+    const float4 q = cell(i, j, k);
+    const real cv = (real)q.w;
+    c[id] = cv;
+    if (j == R.js) c[id - G.sy] = cv;
+    if (j == R.je) c[id + G.sy] = cv;
+    if (k == R.ks) {
+        c[id - 1] = cv;
+        if (j == R.js) c[id - G.sy - 1] = cv;
+        if (j == R.je) c[id + G.sy - 1] = cv;
+    }
+    if (k == R.ke) {
+        c[id + 1] = cv;
+        if (j == R.js) c[id - G.sy + 1] = cv;
+        if (j == R.je) c[id + G.sy + 1] = cv;
+    }
+    if (i > R.is) u[id] = (real)(0.5f * (cell(i - 1, j, k).x + q.x));
+    if (j > R.js) v[id] = (real)(0.5f * (cell(i, j - 1, k).y + q.y));
+    if (k > R.ks) w[id] = (real)(0.5f * (cell(i, j, k - 1).z + q.z));
 }
 
 constexpr int NMID = 14;
@@ -419,6 +458,50 @@ int findmax_t(pllgpu_ctx* ctx, double* val, int* loc, long* nan_at)
 // C ABI
 // ---------------------------------------------------------------------------
 extern "C" {
+
+int pllgpu_pack_cells(pllgpu_ctx* ctx, float* d_cells)
+{
+    if (!ctx || !d_cells || ((uintptr_t)d_cells & 15)) return PLLGPU_EINVAL;
+    CK(cudaSetDevice(ctx->dev));
+    const Rng& R = ctx->Rg;
+    const void* f[4] = {field_ptr(ctx, PLLGPU_U_NEW, false), field_ptr(ctx, PLLGPU_V_NEW, false),
+                        field_ptr(ctx, PLLGPU_W_NEW, false), field_ptr(ctx, PLLGPU_C_NEW, false)};
+    if (!f[0] || !f[1] || !f[2] || !f[3]) return fail(ctx, PLLGPU_ECUDA);
+    const int ni = R.ie - R.is + 1, nj = R.je - R.js + 1, nk = R.ke - R.ks + 1;
+    const long total = (long)ni * nj * nk;
+    const unsigned blocks = (unsigned)((total + 255) / 256);
+    if (ctx->mixed)
+        k_pack_caf<float><<<blocks, 256, 0, ctx->st>>>(ctx->G, (const float*)f[0], (const float*)f[1],
+                                                       (const float*)f[2], (const float*)f[3], R.is, R.js, R.ks, 1,
+                                                       ni, nj, nk, d_cells);
+    else
+        k_pack_caf<double><<<blocks, 256, 0, ctx->st>>>(ctx->G, (const double*)f[0], (const double*)f[1],
+                                                        (const double*)f[2], (const double*)f[3], R.is, R.js, R.ks, 1,
+                                                        ni, nj, nk, d_cells);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->st));
+    return PLLGPU_OK;
+}
+
+int pllgpu_unpack_cells(pllgpu_ctx* ctx, const float* d_cells)
+{
+    if (!ctx || !d_cells || ((uintptr_t)d_cells & 15)) return PLLGPU_EINVAL;
+    CK(cudaSetDevice(ctx->dev));
+    void* f[4] = {field_ptr(ctx, PLLGPU_C_NEW, true), field_ptr(ctx, PLLGPU_U_NEW, true),
+                  field_ptr(ctx, PLLGPU_V_NEW, true), field_ptr(ctx, PLLGPU_W_NEW, true)};
+    if (!f[0] || !f[1] || !f[2] || !f[3]) return fail(ctx, PLLGPU_ECUDA);
+    const Rng& R = ctx->Rg;
+    const dim3 grid((unsigned)((R.ke - R.ks + 1 + 127) / 128), R.je - R.js + 1, R.ie - R.is + 1);
+    if (ctx->mixed)
+        k_unpack_cells<float><<<grid, 128, 0, ctx->st>>>(ctx->G, R, (const float4*)d_cells, (float*)f[0],
+                                                         (float*)f[1], (float*)f[2], (float*)f[3]);
+    else
+        k_unpack_cells<double><<<grid, 128, 0, ctx->st>>>(ctx->G, R, (const float4*)d_cells, (double*)f[0],
+                                                          (double*)f[1], (double*)f[2], (double*)f[3]);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->st));
+    return PLLGPU_OK;
+}
 
 int pllgpu_write_snapshot_ex(pllgpu_ctx* ctx, int fileno, int rank, const char* dir, int subsample)
 {

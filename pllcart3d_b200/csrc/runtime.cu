@@ -478,6 +478,46 @@ int pllgpu_set_tuning(pllgpu_ctx* ctx, int explicit_variant, int line_variant)
     return PLLGPU_OK;
 }
 
+int pllgpu_copy_state(pllgpu_ctx* dst, pllgpu_ctx* src)
+{
+    if (!dst || !src || dst == src || dst->mixed != src->mixed || dst->nelem != src->nelem ||
+        dst->P.nx != src->P.nx || dst->P.ny != src->P.ny || dst->P.nz != src->P.nz)
+        return PLLGPU_EINVAL;
+    pllgpu_ctx* ctx = src;   // error reports go to the source context
+    CK(cudaSetDevice(src->dev));
+    CK(cudaStreamSynchronize(dst->st));
+    const size_t esz = src->mixed ? sizeof(float) : sizeof(double);
+    const size_t bytes = esz * (size_t)src->nelem;
+    auto cp = [&](void* d, const void* s, size_t n) {
+        return cudaMemcpyAsync(d, s, n, cudaMemcpyDeviceToDevice, src->st);
+    };
+    cudaError_t e = cudaSuccess;
+    // both forms keep the same set of arrays; copy buffer for buffer
+    auto copy_bufs = [&](auto& D, auto& S) {
+        for (int v = 0; v < 4; ++v)
+            for (int b = 0; b < 2; ++b) {
+                if (e == cudaSuccess) e = cp(D.q[v][b], S.q[v][b], bytes);
+                if (e == cudaSuccess) e = cp(D.H[v][b], S.H[v][b], bytes);
+            }
+        for (int b = 0; b < 2; ++b)
+            for (int m = 0; m < 4; ++m)
+                if (e == cudaSuccess) e = cp(D.mu[b][m], S.mu[b][m], bytes);
+        for (int v = 1; v < 4; ++v)
+            if (e == cudaSuccess) e = cp(D.pg[v], S.pg[v], bytes);
+        if (e == cudaSuccess) e = cp(D.phi, S.phi, bytes);
+    };
+    if (src->mixed) copy_bufs(dst->b32, src->b32);
+    else copy_bufs(dst->b64, src->b64);
+    if (e == cudaSuccess) e = cp(dst->scal, src->scal, sizeof(double) * S_COUNT);
+    if (e != cudaSuccess) return fail(src, PLLGPU_ECUDA);
+    CK(cudaStreamSynchronize(src->st));
+    dst->cur = src->cur;
+    dst->rotated = src->rotated;
+    dst->resync_c = src->resync_c;
+    dst->timestep = src->timestep;
+    return PLLGPU_OK;
+}
+
 int pllgpu_run_host(pllgpu_ctx* ctx, int nsteps, const double* c0, const double* u0, const double* v0,
                     const double* w0, double* c, double* u, double* v, double* w)
 {

@@ -203,6 +203,32 @@ class Solver:
         sh = p.Subharm if subharm is None else subharm
         self._check(self._L.pllgpu_shift_conc(self._h, float(a), float(lm), int(sh)), "shift_conc")
 
+    # ---- state exchange (learned surrogate, judges) -------------------------
+    def copy_state_from(self, other: "Solver") -> None:
+        """pllgpu_copy_state: this context takes other's whole state."""
+        self._check(self._L.pllgpu_copy_state(self._h, other._h), "copy_state")
+
+    def pack_cells(self, d_ptr: int) -> None:
+        """Cell-centred (u, v, w, c) float32 [nx][ny][nz][4] into device memory."""
+        self._check(self._L.pllgpu_pack_cells(self._h, ctypes.c_void_p(d_ptr)), "pack_cells")
+
+    def unpack_cells(self, d_ptr: int) -> None:
+        self._check(self._L.pllgpu_unpack_cells(self._h, ctypes.c_void_p(d_ptr)), "unpack_cells")
+
+    def project(self) -> None:
+        """The DCT pressure projection of the *_new velocities (divergence,
+        phisolver_dct, velo_correction with its outflow flux fix, ghost
+        fills), then mu from c_new and the new -> old rotation: the state a
+        step starts from.  With dt*alpha = 1 the correction is u - grad
+        lap^-1 div u whatever the time step."""
+        self._routine("divergence")
+        self._routine("phisolver", 1.0, 1.0, 0.0)
+        self._routine("phi_ghosts")
+        self._routine("velo_correction", 1.0, 1.0, 0.0)
+        self._routine("velo_ghosts")
+        self._routine("viscosity_new")
+        self._routine("rotate")
+
     def autotune(self, trial_steps: int = 2) -> int:
         """pllgpu_autotune: picks the fastest launch shapes on steps of this
         run (bit-identical variants); returns the steps it advanced."""
