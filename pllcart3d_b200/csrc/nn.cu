@@ -422,14 +422,31 @@ __global__ void k_mse(const float* __restrict__ P, const float* __restrict__ T, 
     if ((threadIdx.x & 31) == 0 && loss) atomicAdd(loss, s);
 }
 
-// Adam (Kingma & Ba 2015) on FP32 master weights, BF16 copy out
+// sum of squares of x into *out (global gradient norm for clipping)
+__global__ void k_sumsq(const float* __restrict__ x, long n, float* __restrict__ out)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    float s = i < n ? x[i] * x[i] : 0.f;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
+// Adam (Kingma & Ba 2015) on FP32 master weights, BF16 copy out; with
+// sumsq given, the gradient is scaled by min(1, clip / ||g||) (global norm
+// clipping) and a non-finite norm skips the update
 __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
                        float* __restrict__ v, long n, float lr, float b1, float b2, float eps, float bc1, float bc2,
-                       bf16* __restrict__ w16)
+                       bf16* __restrict__ w16, const float* __restrict__ sumsq, float clip)
 {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float gi = g[i];
+    float scale = 1.f;
+    if (sumsq) {
+        const float nrm = sqrtf(*sumsq);
+        if (!isfinite(nrm)) return;
+        if (nrm > clip) scale = clip / nrm;
+    }
+    const float gi = g[i] * scale;
     const float mi = b1 * m[i] + (1.f - b1) * gi;
     const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
     m[i] = mi;
@@ -608,10 +625,17 @@ int pllnn_mse(const float* P, const float* T, long n, float scale, float* grad, 
 }
 
 int pllnn_adam(float* w, const float* g, float* m, float* v, long n, float lr, float b1, float b2, float eps, int t,
-               void* w16, void* stream)
+               void* w16, const float* sumsq, float clip, void* stream)
 {
     const float bc1 = 1.f - powf(b1, (float)t), bc2 = 1.f - powf(b2, (float)t);
-    k_adam<<<nblk(n, 256), 256, 0, (cudaStream_t)stream>>>(w, g, m, v, n, lr, b1, b2, eps, bc1, bc2, (bf16*)w16);
+    k_adam<<<nblk(n, 256), 256, 0, (cudaStream_t)stream>>>(w, g, m, v, n, lr, b1, b2, eps, bc1, bc2, (bf16*)w16,
+                                                           sumsq, clip);
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+int pllnn_sumsq(const float* x, long n, float* out, void* stream)
+{
+    k_sumsq<<<nblk(n, 256), 256, 0, (cudaStream_t)stream>>>(x, n, out);
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 

@@ -67,7 +67,8 @@ def nnlib():
         L.pllnn_cat_fwd.argtypes = [P, I, P, I, Lg, P, P]
         L.pllnn_cat_bwd.argtypes = [P, I, I, Lg, P, I, P, I, P]
         L.pllnn_mse.argtypes = [P, P, Lg, F, P, P, P]
-        L.pllnn_adam.argtypes = [P, P, P, P, Lg, F, F, F, F, I, P, P]
+        L.pllnn_adam.argtypes = [P, P, P, P, Lg, F, F, F, F, I, P, P, F, P]
+        L.pllnn_sumsq.argtypes = [P, Lg, P, P]
         L.pllnn_cast.argtypes = [P, Lg, P, P]
         L.pllnn_pack_input.argtypes = [P, Lg, F, F, P, P, P]
         L.pllnn_pack_target.argtypes = [P, P, Lg, P, P, P]
@@ -233,13 +234,23 @@ class UNet:
             c.gw.zero_()
             c.gb.zero_()
 
-    def adam(self, lr, b1=0.9, b2=0.999, eps=1e-8):
+    def adam(self, lr, b1=0.9, b2=0.999, eps=1e-8, clip=1.0):
+        """One Adam step with global gradient-norm clipping at `clip`
+        (norm reduced on the device; a non-finite norm skips the step)."""
+        import torch
+
         L, st = nnlib(), _stream()
         self.t += 1
+        if not hasattr(self, "_sumsq"):
+            self._sumsq = torch.zeros(1, dtype=torch.float32, device="cuda")
+        self._sumsq.zero_()
+        for c in self.layers.values():
+            for (w, g, m, v) in c.params():
+                _ok(L.pllnn_sumsq(_p(g), g.numel(), _p(self._sumsq), st), "sumsq")
         for c in self.layers.values():
             for (w, g, m, v), w16 in zip(c.params(), (c.w16, None)):
-                _ok(L.pllnn_adam(_p(w), _p(g), _p(m), _p(v), w.numel(), lr, b1, b2, eps, self.t, _p(w16), st),
-                    "adam")
+                _ok(L.pllnn_adam(_p(w), _p(g), _p(m), _p(v), w.numel(), lr, b1, b2, eps, self.t, _p(w16),
+                                 _p(self._sumsq), clip, st), "adam")
             _ok(L.pllnn_flip(_p(c.w16), c.cout, c.k ** 3, c.cin, _p(c.wf16), st), "flip")
 
     def state_dict(self):
@@ -424,34 +435,78 @@ def rel(a, b):
 
 
 def rollout(sur: Surrogate, wl, steps=2000, judge_every=4, tol=1e-3, precision="fp64"):
-    """Surrogate + judge rollout of `steps` steps; returns a report."""
+    """Surrogate + judge rollout of `steps` steps; returns a report.
+
+    Windows of 8 steps.  Every `judge_every`-th window the plain solver runs
+    the same window from the same start on a second context; the surrogate
+    window is rejected (the solver's state taken) when mass or mixing length
+    differ by more than `tol`.  A non-finite prediction is always replaced
+    by a solver window; when the state reached through accepted windows makes
+    the solver itself fail, the rollout goes back to the last state a judge
+    verified and the solver runs every window since."""
     import torch
 
+    from . import _lib
     from .ic import workload_fields
     from .solver import Solver
 
     R, Pe = -wl.params.Vratio, wl.params.Pe
     ic = workload_fields(wl)
-    S = Solver(wl.params, precision=precision)
-    J = Solver(wl.params, precision=precision)
-    S.load_ic(ic)
-    J.load_ic(ic)
+    S = Solver(wl.params, precision=precision)       # the rollout state
+    J = Solver(wl.params, precision=precision)       # the judge
+    Sprev = Solver(wl.params, precision=precision)   # start of the window
+    Sgood = Solver(wl.params, precision=precision)   # last verified state
+    for x in (S, J, Sprev, Sgood):
+        x.load_ic(ic)
+    wgood = 0
     nwin = steps // WINDOW
-    judged = rejected = 0
+    judged = rejected = failed = broken = 0
+    trace = []
+
+    def solver_window(start):
+        """The solver's window from `start` into J; False when the start
+        state makes the solver fail (NaN/Inf)."""
+        J.copy_state_from(start)
+        try:
+            J.step(WINDOW)
+            return True
+        except _lib.PllGpuError:
+            J.clear_status()
+            return False
+
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for w in range(nwin):
         judge = (w % judge_every) == judge_every - 1
-        if judge:
-            J.copy_state_from(S)
-            J.step(WINDOW)
+        Sprev.copy_state_from(S)
+        judged_ok = solver_window(S) if judge else False
         sur.advance(S, R, Pe)
-        if judge:
-            judged += 1
-            ds, dj = S.diagnostics(), J.diagnostics()
+        ds = S.diagnostics()
+        if not all(math.isfinite(x) for x in ds.values()):
+            failed += 1
+            if not judged_ok and not solver_window(Sprev):
+                raise RuntimeError(f"window {w}: the solver fails from the accepted state")
+            S.copy_state_from(J)
+            continue
+        if not judge:
+            continue
+        judged += 1
+        if not judged_ok:
+            rejected += 1
+            broken += 1
+            J.copy_state_from(Sgood)
+            J.step(WINDOW * (w + 1 - wgood))
+            S.copy_state_from(J)
+        else:
+            dj = J.diagnostics()
+            if len(trace) < 16:
+                trace.append({"window": w, "mass_rel": rel(ds["mass"], dj["mass"]),
+                              "ml": ds["mixing_length"], "ml_solver": dj["mixing_length"]})
             if rel(ds["mass"], dj["mass"]) > tol or rel(ds["mixing_length"], dj["mixing_length"]) > tol:
                 rejected += 1
                 S.copy_state_from(J)
+        Sgood.copy_state_from(S)
+        wgood = w + 1
     torch.cuda.synchronize()
     t_roll = time.perf_counter() - t0
     # the plain FP64 run of the same steps
@@ -467,6 +522,7 @@ def rollout(sur: Surrogate, wl, steps=2000, judge_every=4, tol=1e-3, precision="
     c_err = float(np.abs(S.get("c_new") - P.get("c_new")).max())
     return {"steps": steps, "windows": nwin, "judged": judged, "rejected": rejected,
             "accepted_fraction_of_judged": (judged - rejected) / max(judged, 1),
+            "nonfinite_windows": failed, "judge_failed_windows": broken, "judge_trace": trace,
             "mixing_length": ds["mixing_length"], "mixing_length_plain": dp["mixing_length"],
             "mixing_length_rel_error": rel(ds["mixing_length"], dp["mixing_length"]),
             "mass_rel_error": rel(ds["mass"], dp["mass"]), "c_maxnorm_error": c_err,
@@ -481,7 +537,7 @@ def main(argv=None) -> int:
     ap.add_argument("--data-steps", type=int, default=400)
     ap.add_argument("--train-steps", type=int, default=2000)
     ap.add_argument("--batch", type=int, default=8)
-    ap.add_argument("--lr", type=float, default=3e-4)
+    ap.add_argument("--lr", type=float, default=2e-4)
     ap.add_argument("--rollout", type=int, default=2000)
     ap.add_argument("--grid", default="128x64x64")
     ap.add_argument("--save", default=None)
@@ -490,7 +546,7 @@ def main(argv=None) -> int:
     t0 = time.perf_counter()
     ds, wls = generate_data(args.runs, grid, args.data_steps)
     t_data = time.perf_counter() - t0
-    # hold out the last run for evaluation
+    # hold out the last run for evaluation and the rollout
     per_run = len(ds.a) // args.runs
     held = list(range(len(ds.a) - per_run, len(ds.a)))
     train_idx = np.arange(0, len(ds.a) - per_run)
@@ -498,22 +554,30 @@ def main(argv=None) -> int:
     tr = Trainer(net, ds, batch=args.batch, lr=args.lr)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
+    curve = []
     for s in range(args.train_steps):
+        log = s % 250 == 0 or s == args.train_steps - 1
+        if log:
+            tr.loss.zero_()
         tr.step(tr.rng.choice(train_idx, args.batch))
+        if log:
+            curve.append((s, float(tr.loss.item())))
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t1
     loss, loss0 = tr.eval_loss(held[::max(1, len(held) // 8)])
+    if args.save:
+        sd = net.state_dict()
+        np.savez(args.save, norm=tr.norm, dscale=tr.dscale, **{f"{n}_w": w for n, (w, b) in sd.items()},
+                 **{f"{n}_b": b for n, (w, b) in sd.items()})
+    print(json.dumps({"phase": "trained", "train_s": t_train, "heldout_mse": loss,
+                      "heldout_mse_persistence": loss0, "loss_curve": curve}), flush=True)
     sur = Surrogate(net, tr.norm, tr.dscale, grid)
-    # the rollout runs the held-out member (never seen in training)
     rep = rollout(sur, wls[-1], args.rollout)
     rep.update({"grid": list(grid), "params": net.n_params(), "train_steps": args.train_steps,
                 "batch": args.batch, "train_s": t_train, "train_ms_per_step": 1e3 * t_train / max(1, args.train_steps),
-                "data_s": t_data, "samples": len(ds.a), "heldout_mse": loss, "heldout_mse_persistence": loss0})
+                "data_s": t_data, "samples": len(ds.a), "heldout_mse": loss, "heldout_mse_persistence": loss0,
+                "loss_curve": curve})
     print(json.dumps(rep))
-    if args.save:
-        np.savez(args.save, norm=tr.norm, dscale=tr.dscale,
-                 **{f"{n}_w": w for n, (w, b) in net.state_dict().items()},
-                 **{f"{n}_b": b for n, (w, b) in net.state_dict().items()})
     return 0
 
 

@@ -93,7 +93,7 @@ def test_pool_up_cat_adam():
     for t in range(1, 4):
         gr = rng.standard_normal(1000)
         assert L.pllnn_adam(S._p(w32), S._p(_t(gr, torch.float32)), S._p(m), S._p(v), 1000, 1e-2, 0.9, 0.999, 1e-8,
-                            t, None, st) == 0
+                            t, None, None, 0.0, st) == 0
         wr, mr, vr = nn_ref.adam(wr, gr, mr, vr, 1e-2, 0.9, 0.999, 1e-8, t)
     assert _relerr(w32.cpu().numpy(), wr) < 1e-5
 
@@ -146,5 +146,5 @@ def test_training_beats_persistence():
     for _ in range(300):
         tr.step(tr.rng.choice(train, 4))
     after, persist2 = tr.eval_loss(held)
-    assert persist == pytest.approx(persist2)
+    assert persist == pytest.approx(persist2, rel=1e-5)   # FP32 atomics: order varies
     assert after < 0.5 * persist, (before, after, persist)
