@@ -18,8 +18,9 @@ larger than the 126 MB L2, so no L2 flush is needed between steps.
                   pllgpu_run_host with pinned host buffers (initial fields
                   in, c/u/v/w out, inside the timed region).
 --impl reference  the reference's own CPU step (pllcart3d.c compiled by
-                  oracle/Makefile, single rank), timed on the host cores on a
-                  bounded sample of steps of the same workload.
+                  oracle/Makefile, single rank), one process per host core,
+                  each timed on a bounded sample of steps of the same
+                  workload's physics; cell-steps/s summed over the cores.
 With N>1 (torchrun) every rank advances its own replica (the north-star path
 runs on one GPU; replicas only) and `value` sums cells over ranks.
 """
@@ -39,7 +40,7 @@ from pllcart3d_b200 import roofline  # noqa: E402
 from pllcart3d_b200.ic import workload_fields  # noqa: E402
 from pllcart3d_b200.params import workload  # noqa: E402
 
-METRIC = "cell-steps/s"
+METRIC = "cell-steps/s: mixed vs plain FP64 on 1 B200 at \u22641e-5 c error; surrogate speedup"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
@@ -75,14 +76,22 @@ def dist_setup():
 
 
 def reduce_max(x, ws):
+    """Max of x over the ranks (the slowest replica's time)."""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(cells, steps, ws, ms_max):
+    """Whole-job throughput of ws replicas: every rank advances its own copy
+    of the workload, timed as the slowest rank."""
+    return cells * steps * ws / (ms_max / 1e3)
 
 
 def barrier(ws):
@@ -179,16 +188,35 @@ def cpu_sample(wl_name, seconds=12.0):
     return cells * n / dt, kind, sample, n
 
 
+def _ref_worker(wl_name, seconds, q):
+    v, kind, sample, n = cpu_sample(wl_name, seconds=seconds)
+    q.put((v, kind, sample))
+
+
 def run_reference(args, ws, rank):
+    """The reference's own CPU step on every host core: one single-rank
+    reference process per core (independent replicas, no communication, so
+    an upper bound on what its MPI decomposition reaches on these cores),
+    each a bounded sample of the workload; cell-steps/s summed over cores."""
     if rank != 0:
         return
+    import multiprocessing as mp
+
     wl = workload(args.workload)
-    vals = []
-    # warm-up and timed steps, each a bounded sample of the workload
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    vals, kind, sample = [], "reference", ""
     for s in range(args.warmup + args.steps):
-        v, kind, sample, n = cpu_sample(args.workload, seconds=2.0)
+        q = ctx.Queue()
+        procs = [ctx.Process(target=_ref_worker, args=(args.workload, 2.0, q)) for _ in range(cores)]
+        for p in procs:
+            p.start()
+        res = [q.get(timeout=600) for _ in procs]
+        for p in procs:
+            p.join(timeout=60)
+        kind, sample = res[0][1], res[0][2]
         if s >= args.warmup:
-            vals.append(v)
+            vals.append(sum(r[0] for r in res))
     value = statistics.mean(vals)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-steps/s",
@@ -197,8 +225,8 @@ def run_reference(args, ws, rank):
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": wl.name, "grid": [wl.params.nx, wl.params.ny, wl.params.nz],
                    "precision": "fp64"},
-        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": 1,
-                         "kind": kind, "sample": sample + " per step"},
+        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": cores, "kind": kind,
+                         "sample": f"{cores} processes, each: " + sample + " per step"},
         "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -246,20 +274,58 @@ def measure(prm, ic, form, steps, warmup, ws, local, profile_steps=2):
     return out
 
 
-def roofline_of(kernels, nprof, cells, precision):
+def tensor_peak():
+    """Dense TF32 tensor peak: half the measured BF16 GEMM rate (B200 runs
+    TF32 at half the BF16 rate); None without a measurement."""
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["bf16_tflops"]) / 2.0
+    except Exception:
+        return None
+
+
+# DRAM bytes per cell of one launch, from the ncu captures in profiles/
+# (256x128x128 case; the kernels' traffic grows with the cells processed)
+TRAFFIC_PER_CELL = {}
+
+
+def roofline_of(kernels, nprof, cells, precision, dims=None):
+    """Roofline of the kernel family with the largest share of the step."""
     hbm, peak_kind = peaks()
-    cand = {k: v for k, v in kernels.items() if k in roofline.KERNEL_WORDS}
-    if not cand:
+    fam = {}
+    for lab, v in kernels.items():
+        f = roofline.FAMILY.get(lab)
+        if f is None:
+            continue
+        d = fam.setdefault(f, {"ms": 0.0, "launches": 0, "bytes": 0.0, "labels": []})
+        d["ms"] += v["ms_total"]
+        d["launches"] += v["launches"]
+        d["bytes"] += roofline.kernel_bytes_per_launch(lab, cells, precision) * v["launches"]
+        d["labels"].append(lab)
+    if not fam:
         return None
     step_ms_prof = sum(v["ms_total"] for v in kernels.values()) / nprof
-    top = max(cand, key=lambda k: cand[k]["ms_total"])
-    avg_ms = cand[top]["ms_total"] / cand[top]["launches"]
-    alg = roofline.kernel_bytes_per_launch(top, cells, precision)
+    top = max(fam, key=lambda f: fam[f]["ms"])
+    d = fam[top]
+    avg_ms = d["ms"] / d["launches"]
+    out = {"kernel": top, "labels": sorted(d["labels"]), "avg_launch_ms": avg_ms,
+           "share_of_step": d["ms"] / nprof / step_ms_prof, "peak_source": peak_kind}
+    tens = [lab for lab in d["labels"] if lab in roofline.TENSOR_PASS_FLOPS]
+    if tens and dims is not None:
+        nx, ny, nz = dims
+        flops = roofline.TENSOR_PASS_FLOPS[tens[0]] * (ny + nz) * cells   # mean pass: 2n flops/cell
+        ach = flops / (avg_ms / 1e3) / 1e12
+        pk = tensor_peak()
+        out.update({"bound": "tensor", "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                    "frac": ach / pk if pk else None, "traffic": None,
+                    "algorithmic_flops_per_launch": flops})
+        return out
+    alg = d["bytes"] / d["launches"]
     ach = alg / (avg_ms / 1e3) / 1e9
-    return {"kernel": top, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-            "frac": ach / hbm, "traffic": None, "peak_source": peak_kind,
-            "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
-            "share_of_step": cand[top]["ms_total"] / nprof / step_ms_prof}
+    tpc = TRAFFIC_PER_CELL.get((top, precision))
+    out.update({"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "traffic": tpc * cells if tpc else None, "algorithmic_bytes_per_launch": alg})
+    return out
 
 
 def run_ours(args, ws, rank, local):
@@ -282,8 +348,8 @@ def run_ours(args, ws, rank, local):
         m = measure(prm, ic, form, args.steps, args.warmup, ws, local)
         prec = "fp32" if form == "mixed" else "fp64"
         sb = roofline.step_bytes(cells, prec)
-        m["value"] = cells * args.steps * ws / (m["ms"] / 1e3)
-        m["roofline"] = roofline_of(m["kernels"], m["profile_steps"], cells, prec)
+        m["value"] = replica_value(cells, args.steps, ws, m["ms"])
+        m["roofline"] = roofline_of(m["kernels"], m["profile_steps"], cells, prec, (prm.nx, prm.ny, prm.nz))
         m["step_roofline"] = {"bytes_per_step": sb,
                               "achieved_gbs": sb / (m["ms"] / args.steps / 1e3) / 1e9,
                               "frac_of_hbm": sb / (m["ms"] / args.steps / 1e3) / 1e9 / hbm}
@@ -345,7 +411,9 @@ def run_ours(args, ws, rank, local):
         for form, m in forms.items():
             line[f"{form}_form"] = {"value": m["value"], "ms_per_step": m["ms"] / args.steps,
                                     "step_roofline_frac": m["step_roofline"]["frac_of_hbm"],
-                                    "roofline": m["roofline"], "clocks": m["clocks"]}
+                                    "roofline": m["roofline"], "clocks": m["clocks"],
+                                    "kernels_ms_per_step": {k: v["ms_total"] / m["profile_steps"]
+                                                            for k, v in m["kernels"].items()}}
         if "fp64" in forms and "mixed" in forms:
             line["mixed_over_fp64"] = forms["mixed"]["value"] / forms["fp64"]["value"]
         print(json.dumps(line), flush=True)

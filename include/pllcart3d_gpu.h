@@ -345,6 +345,8 @@ int pllgpu_dct2d_batch_noalloc(int kind, int n0, int n1, int howmany,
 /*   int  pllgpu_advance(int nsteps,double *tval);                          */
 /*   int  pllgpu_sync_to_host(void);                                        */
 /*   int  pllgpu_dropin_status(void); void pllgpu_finalize(void);           */
+/*   pllgpu_ctx *pllgpu_dropin_context(void);  the context behind attach,   */
+/*        for the resident snapshot / restart / diagnostic calls above      */
 /* Layout-identical mirrors of the reference types follow.                   */
 /* ------------------------------------------------------------------------ */
 typedef struct pll_tds {          /* Tds, structures_3d.h:2-8 */

@@ -550,6 +550,12 @@ int pllgpu_advance(int nsteps, double *tval)
     return PLLGPU_OK;
 }
 
+/* the device context behind pllgpu_attach, for the resident output calls
+ * (pllgpu_write_snapshot, pllgpu_write_restart, pllgpu_conc_average,
+ * pllgpu_find_max, pllgpu_find_wmax, pllgpu_shift_conc) that replace the
+ * reference's file output without a copy of the state to the host */
+pllgpu_ctx *pllgpu_dropin_context(void) { return g_ctx; }
+
 /* state back into the attached host arrays (before any of the reference's
  * file output or diagnostics, pllcart3d.c:198-256) */
 int pllgpu_sync_to_host(void)

@@ -29,10 +29,31 @@ KERNEL_WORDS = {
     "viscosity": 5,      # c ; 4 viscosity families
     "div_rhs": 4,        # u, v, w ; rhs
     "dct_gemm": 2,       # one dense pass: in ; out (per launch)
+    "dct_umma": 2,
     "poisson_x": 2,
     "project": 17,       # u v w phi mu(4) pg(3) ; u v w pg(3)
     "cfl": 3,
 }
+
+
+# kernel families (one CUDA kernel template each) of the per-launch labels
+FAMILY = {
+    "explicit_c": "k_explicit", "explicit_u": "k_explicit", "explicit_v": "k_explicit",
+    "explicit_w": "k_explicit",
+    "adi_y_c": "k_line_pf (y)", "adi_y_u": "k_line_pf (y)", "adi_y_v": "k_line_pf (y)",
+    "adi_y_w": "k_line_pf (y)",
+    "adi_z_c": "k_adi_z_tiled", "adi_z_u": "k_adi_z_tiled", "adi_z_v": "k_adi_z_tiled",
+    "adi_z_w": "k_adi_z_tiled",
+    "adi_x_c": "k_line_pf (x)", "adi_x_u": "k_line_pf (x)", "adi_x_v": "k_line_pf (x)",
+    "adi_x_w": "k_line_pf (x)",
+    "viscosity": "k_viscosity", "div_rhs": "k_div_rhs", "dct_gemm": "k_gemm_dmma",
+    "dct_umma": "k_dct_umma", "poisson_x": "k_poisson_x", "project": "k_project", "cfl": "k_cfl",
+}
+
+# tensor-core kernels: products per DCT pass (one dense product of 2 n flops
+# per cell for a pass of length n; the precision form's split-TF32 passes
+# issue 3: hi*hi, hi*lo, lo*hi)
+TENSOR_PASS_FLOPS = {"dct_gemm": 1, "dct_umma": 3}
 
 
 def kernel_bytes_per_launch(label: str, cells: int, precision: str = "fp64") -> float:

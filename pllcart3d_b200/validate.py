@@ -1,12 +1,17 @@
-"""Accuracy of the precision form against the plain FP64 step.
+"""Accuracy of one form of the step against another (default: the precision
+form against the plain FP64 step).
 
     python -m pllcart3d_b200.validate [--workload NAME] [--steps N] [--every K]
+                                      [--test FORM] [--ref FORM]
 
-Both forms start from the same seeded initial condition and advance in
-lockstep; every K steps the relative max-norm error of each field of the
-precision form (max|mixed - fp64| / max|fp64| over the padded box) and the
-FP64 diagnostics of both (mass, divergence norms, mixing length) are
-printed, one JSON line per checkpoint.
+FORM: fp64 (DMMA DCT), fp64-exact (sequential-order DCT), mixed (tcgen05
+split-TF32 DCT where the shape allows), mixed-mma (mma.sync split-TF32 DCT),
+mixed-seq (sequential FP32 DCT).  Both runs start from the same seeded
+initial condition and advance in lockstep; every K steps (or at the steps
+listed by --at) the relative max-norm error of each field (velocity
+components against the velocity vector's max-norm) and the FP64 diagnostics
+of both (mass, divergence norms, mixing length) are printed, one JSON line
+per checkpoint.
 """
 
 from __future__ import annotations
@@ -22,11 +27,18 @@ from .params import workload
 from .solver import Solver
 
 FIELDS = ("c_new", "u_new", "v_new", "w_new", "phi", "u_pg", "v_pg", "w_pg")
+VECTORS = {"u_new": ("u_new", "v_new", "w_new"), "v_new": ("u_new", "v_new", "w_new"),
+           "w_new": ("u_new", "v_new", "w_new"), "u_pg": ("u_pg", "v_pg", "w_pg"),
+           "v_pg": ("u_pg", "v_pg", "w_pg"), "w_pg": ("u_pg", "v_pg", "w_pg")}
+FORMS = {"fp64": dict(precision="fp64"), "fp64-exact": dict(precision="fp64", exact_dct=True),
+         "mixed": dict(precision="mixed"), "mixed-mma": dict(precision="mixed", dct_kernel="mma_sync"),
+         "mixed-seq": dict(precision="mixed", exact_dct=True)}
 
 
-def rel(a: np.ndarray, b: np.ndarray) -> float:
-    den = float(np.abs(b).max())
-    return float(np.abs(a - b).max()) / den if den > 0 else float(np.abs(a - b).max())
+def rel(test, ref, f) -> float:
+    den = max(float(np.abs(ref.get(c)).max()) for c in VECTORS.get(f, (f,)))
+    num = float(np.abs(test.get(f) - ref.get(f)).max())
+    return num / den if den > 0 else num
 
 
 def main(argv=None) -> int:
@@ -35,17 +47,22 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--every", type=int, default=250)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--test", default="mixed", choices=sorted(FORMS))
+    ap.add_argument("--ref", default="fp64", choices=sorted(FORMS))
+    ap.add_argument("--at", default=None, help="comma-separated checkpoint steps (instead of --every)")
     args = ap.parse_args(argv)
     wl = workload(args.workload)
     ic = workload_fields(wl)
-    ref = Solver(wl.params, device=args.device, precision="fp64")
-    mix = Solver(wl.params, device=args.device, precision="mixed")
+    ref = Solver(wl.params, device=args.device, **FORMS[args.ref])
+    mix = Solver(wl.params, device=args.device, **FORMS[args.test])
+    marks = sorted(int(t) for t in args.at.split(",")) if args.at else None
     ref.load_ic(ic)
     mix.load_ic(ic)
     done = 0
     t_ref = t_mix = 0.0
-    while done < args.steps:
-        n = min(args.every, args.steps - done)
+    last = marks[-1] if marks else args.steps
+    while done < last:
+        n = (next(m for m in marks if m > done) - done) if marks else min(args.every, args.steps - done)
         t0 = time.perf_counter()
         ref.step(n)
         t1 = time.perf_counter()
@@ -54,11 +71,11 @@ def main(argv=None) -> int:
         t_ref += t1 - t0
         t_mix += t2 - t1
         done += n
-        errs = {f: rel(mix.get(f), ref.get(f)) for f in FIELDS}
-        line = {"workload": wl.name, "steps": done, "rel_maxnorm": errs,
-                "diag_fp64": ref.diagnostics(), "diag_mixed": mix.diagnostics(),
-                "dt_fp64": ref.dt, "dt_mixed": mix.dt, "tval_fp64": ref.tval,
-                "tval_mixed": mix.tval, "wall_s_fp64": t_ref, "wall_s_mixed": t_mix}
+        errs = {f: rel(mix, ref, f) for f in FIELDS}
+        line = {"workload": wl.name, "test": args.test, "ref": args.ref, "steps": done,
+                "rel_maxnorm": errs, "diag_ref": ref.diagnostics(), "diag_test": mix.diagnostics(),
+                "dt_ref": ref.dt, "dt_test": mix.dt, "tval_ref": ref.tval, "tval_test": mix.tval,
+                "wall_s_ref": t_ref, "wall_s_test": t_mix}
         print(json.dumps(line), flush=True)
     return 0
 
