@@ -439,11 +439,11 @@ def rollout(sur: Surrogate, wl, steps=2000, judge_every=4, tol=1e-3, precision="
 
     Windows of 8 steps.  Every `judge_every`-th window the plain solver runs
     the same window from the same start on a second context; the surrogate
-    window is rejected (the solver's state taken) when mass or mixing length
-    differ by more than `tol`.  A non-finite prediction is always replaced
-    by a solver window; when the state reached through accepted windows makes
-    the solver itself fail, the rollout goes back to the last state a judge
-    verified and the solver runs every window since."""
+    window is rejected when mass or mixing length differ by more than `tol`
+    (or the solver cannot step from that start).  A rejection, or a
+    non-finite prediction anywhere, sends the rollout back to the last state
+    a judge verified, and the solver runs every window since: the state is
+    verified at every judged window."""
     import torch
 
     from . import _lib
@@ -454,9 +454,8 @@ def rollout(sur: Surrogate, wl, steps=2000, judge_every=4, tol=1e-3, precision="
     ic = workload_fields(wl)
     S = Solver(wl.params, precision=precision)       # the rollout state
     J = Solver(wl.params, precision=precision)       # the judge
-    Sprev = Solver(wl.params, precision=precision)   # start of the window
     Sgood = Solver(wl.params, precision=precision)   # last verified state
-    for x in (S, J, Sprev, Sgood):
+    for x in (S, J, Sgood):
         x.load_ic(ic)
     wgood = 0
     nwin = steps // WINDOW
@@ -474,39 +473,46 @@ def rollout(sur: Surrogate, wl, steps=2000, judge_every=4, tol=1e-3, precision="
             J.clear_status()
             return False
 
+    def fall_back(w):
+        """Rejection: back to the last verified state; the solver runs every
+        window since (the result is verified by construction)."""
+        nonlocal wgood
+        J.copy_state_from(Sgood)
+        J.step(WINDOW * (w + 1 - wgood))
+        S.copy_state_from(J)
+        Sgood.copy_state_from(S)
+        wgood = w + 1
+
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for w in range(nwin):
         judge = (w % judge_every) == judge_every - 1
-        Sprev.copy_state_from(S)
         judged_ok = solver_window(S) if judge else False
         sur.advance(S, R, Pe)
         ds = S.diagnostics()
-        if not all(math.isfinite(x) for x in ds.values()):
+        finite = all(math.isfinite(x) for x in ds.values())
+        if not finite:
             failed += 1
-            if not judged_ok and not solver_window(Sprev):
-                raise RuntimeError(f"window {w}: the solver fails from the accepted state")
-            S.copy_state_from(J)
-            continue
         if not judge:
+            if not finite:
+                fall_back(w)
             continue
         judged += 1
-        if not judged_ok:
+        if not judged_ok or not finite:
+            broken += int(not judged_ok)
             rejected += 1
-            broken += 1
-            J.copy_state_from(Sgood)
-            J.step(WINDOW * (w + 1 - wgood))
-            S.copy_state_from(J)
+            fall_back(w)
+            continue
+        dj = J.diagnostics()
+        if len(trace) < 16:
+            trace.append({"window": w, "mass_rel": rel(ds["mass"], dj["mass"]),
+                          "ml": ds["mixing_length"], "ml_solver": dj["mixing_length"]})
+        if rel(ds["mass"], dj["mass"]) > tol or rel(ds["mixing_length"], dj["mixing_length"]) > tol:
+            rejected += 1
+            fall_back(w)
         else:
-            dj = J.diagnostics()
-            if len(trace) < 16:
-                trace.append({"window": w, "mass_rel": rel(ds["mass"], dj["mass"]),
-                              "ml": ds["mixing_length"], "ml_solver": dj["mixing_length"]})
-            if rel(ds["mass"], dj["mass"]) > tol or rel(ds["mixing_length"], dj["mixing_length"]) > tol:
-                rejected += 1
-                S.copy_state_from(J)
-        Sgood.copy_state_from(S)
-        wgood = w + 1
+            Sgood.copy_state_from(S)
+            wgood = w + 1
     torch.cuda.synchronize()
     t_roll = time.perf_counter() - t0
     # the plain FP64 run of the same steps
@@ -541,6 +547,7 @@ def main(argv=None) -> int:
     ap.add_argument("--rollout", type=int, default=2000)
     ap.add_argument("--grid", default="128x64x64")
     ap.add_argument("--save", default=None)
+    ap.add_argument("--load", default=None, help="a network saved by --save: skip training")
     args = ap.parse_args(argv)
     grid = tuple(int(t) for t in args.grid.split("x"))
     t0 = time.perf_counter()
@@ -552,6 +559,13 @@ def main(argv=None) -> int:
     train_idx = np.arange(0, len(ds.a) - per_run)
     net = UNet(seed=0)
     tr = Trainer(net, ds, batch=args.batch, lr=args.lr)
+    if args.load:
+        z = np.load(args.load)
+        net.load_state_dict({n: (z[f"{n}_w"], z[f"{n}_b"]) for n in net.layers})
+        tr.norm, tr.dscale = z["norm"], z["dscale"]
+        tr.norm_t.copy_(torch.tensor(tr.norm))
+        tr.dscale_t.copy_(torch.tensor(tr.dscale))
+        args.train_steps = 0
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     curve = []
