@@ -357,7 +357,9 @@ def run_ours(args, ws, rank, local):
         if form != args.headline:
             m["solver"].close()
 
-    head = forms[args.headline]
+    head = forms[args.headline] if args.headline in forms else forms[args.precision]
+    if args.headline not in forms:
+        args.headline = args.precision
     s = head["solver"]
 
     e2e = None
