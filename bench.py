@@ -284,9 +284,10 @@ def tensor_peak():
         return None
 
 
-# DRAM bytes per cell of one launch, from the ncu captures in profiles/
-# (256x128x128 case; the kernels' traffic grows with the cells processed)
-TRAFFIC_PER_CELL = {}
+# DRAM traffic over algorithmic bytes of a launch, from the ncu captures of
+# the 256x128x128 case (profiles/); traffic grows with the cells processed,
+# so a full launch's traffic is this ratio times its algorithmic bytes
+TRAFFIC_RATIO = {("k_explicit", "fp32"): 1.02, ("k_explicit", "fp64"): 1.04}
 
 
 def roofline_of(kernels, nprof, cells, precision, dims=None):
@@ -322,9 +323,9 @@ def roofline_of(kernels, nprof, cells, precision, dims=None):
         return out
     alg = d["bytes"] / d["launches"]
     ach = alg / (avg_ms / 1e3) / 1e9
-    tpc = TRAFFIC_PER_CELL.get((top, precision))
+    ratio = TRAFFIC_RATIO.get((top, precision))
     out.update({"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                "traffic": tpc * cells if tpc else None, "algorithmic_bytes_per_launch": alg})
+                "traffic": ratio * alg if ratio else None, "algorithmic_bytes_per_launch": alg})
     return out
 
 
