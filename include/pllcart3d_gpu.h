@@ -61,8 +61,9 @@ typedef struct pllgpu_params {
                               the CPU restatement); 0: tensor-core DMMA        */
     int use_graph;         /* 1: replay each step as one CUDA graph            */
     int dct_kernel;        /* precision form, exact_dct 0: 0 = tcgen05 split-TF32
-                              GEMMs where ny, nz are 128 or 256, else mma.sync;
-                              1 = mma.sync split-TF32 always                   */
+                              GEMMs (persistent, one CTA per SM) where ny, nz
+                              are 128 or 256, else mma.sync; 1 = mma.sync
+                              split-TF32 always; 2 = tcgen05, one tile per CTA */
     int reserved[4];
 } pllgpu_params;
 

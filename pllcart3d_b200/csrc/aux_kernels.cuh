@@ -19,7 +19,9 @@ __device__ __forceinline__ real visc_law(real cavg, const Consts& K, int nmvp,
                                          const double* __restrict__ scal)
 {
     if (!nmvp) {
-        if (sizeof(real) == 4) return (real)expf((float)((real)K.M * (cavg - (real)K.Vnorm)));
+        // the precision form: the fast exponential (ex2-based, a few ulp for
+        // the |M (c - Vnorm)| <= ~3 of these runs), FP32-level like its state
+        if (sizeof(real) == 4) return (real)__expf((float)((real)K.M * (cavg - (real)K.Vnorm)));
         return (real)exp((double)((real)K.M * (cavg - (real)K.Vnorm)));
     }
     // calculate_viscosity_nmvp, pllcart3d.c:906-909

@@ -41,6 +41,7 @@ struct Bufs {
 // (A = the data, Bh / Bl = the cosine matrix's TF32 head and tail)
 struct UmmaPlan {
     bool on = false;
+    int sms = 148;   // persistent grid: one CTA per SM
     CUtensorMap a[4], bh[4], bl[4];
     float* Thi[4] = {};
     float* Tlo[4] = {};

@@ -120,13 +120,24 @@ void launch_gemm(pllgpu_ctx* ctx, const GemmDesc& d, const float* A, const float
 void launch_umma(pllgpu_ctx* ctx, int pass, long rows, int K, const UmmaEpi& e, float* out)
 {
     const UmmaPlan& U = ctx->um;
-    const dim3 grid((unsigned)(rows / UM_BM));
-    if (K == 256)
-        k_dct_umma<256><<<grid, UM_THREADS, UmmaSmem<256>::DYN, ctx->st>>>(U.a[pass], U.bh[pass], U.bl[pass], K, e,
-                                                                           out, ctx->status);
-    else
-        k_dct_umma<128><<<grid, UM_THREADS, UmmaSmem<128>::DYN, ctx->st>>>(U.a[pass], U.bh[pass], U.bl[pass], K, e,
-                                                                           out, ctx->status);
+    const int ntiles = (int)(rows / UM_BM);
+    if (ctx->P.dct_kernel == 2) {   // one tile per CTA
+        const dim3 grid((unsigned)ntiles);
+        if (K == 256)
+            k_dct_umma<256><<<grid, UM_THREADS, UmmaSmem<256>::DYN, ctx->st>>>(U.a[pass], U.bh[pass], U.bl[pass],
+                                                                               K, e, out, ctx->status);
+        else
+            k_dct_umma<128><<<grid, UM_THREADS, UmmaSmem<128>::DYN, ctx->st>>>(U.a[pass], U.bh[pass], U.bl[pass],
+                                                                               K, e, out, ctx->status);
+    } else {   // persistent: one CTA per SM
+        const dim3 grid((unsigned)std::min(ntiles, U.sms));
+        if (K == 256)
+            k_dct_umma_p<256><<<grid, UMP_THREADS, UmmaPSmem<256>::DYN, ctx->st>>>(
+                U.a[pass], U.bh[pass], U.bl[pass], K, ntiles, e, out, ctx->status);
+        else
+            k_dct_umma_p<128><<<grid, UMP_THREADS, UmmaPSmem<128>::DYN, ctx->st>>>(
+                U.a[pass], U.bh[pass], U.bl[pass], K, ntiles, e, out, ctx->status);
+    }
     mark(ctx, "dct_umma");
 }
 
@@ -614,7 +625,12 @@ bool setup_umma(pllgpu_ctx* c)
     if (cudaFuncSetAttribute(k_dct_umma<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)UmmaSmem<256>::DYN) != cudaSuccess ||
         cudaFuncSetAttribute(k_dct_umma<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)UmmaSmem<128>::DYN) != cudaSuccess)
+                             (int)UmmaSmem<128>::DYN) != cudaSuccess ||
+        cudaFuncSetAttribute(k_dct_umma_p<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)UmmaPSmem<256>::DYN) != cudaSuccess ||
+        cudaFuncSetAttribute(k_dct_umma_p<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)UmmaPSmem<128>::DYN) != cudaSuccess ||
+        cudaDeviceGetAttribute(&U.sms, cudaDevAttrMultiProcessorCount, c->dev) != cudaSuccess)
         return false;
     U.on = true;
     return true;
@@ -659,7 +675,7 @@ bool alloc_state(pllgpu_ctx* c)
                          (int)adi_z_smem_bytes<VW, real>());
     if constexpr (std::is_same<real, float>::value) {
         const bool shape_ok = (p->ny == 128 || p->ny == 256) && (p->nz == 128 || p->nz == 256);
-        if (shape_ok && !p->exact_dct && p->dct_kernel == 0 && !setup_umma(c)) return false;
+        if (shape_ok && !p->exact_dct && p->dct_kernel != 1 && !setup_umma(c)) return false;
     }
     return true;
 }

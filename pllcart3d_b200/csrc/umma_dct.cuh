@@ -343,5 +343,216 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
     if (threadIdx.x == 0 && *abort_flag) atomicOr(status, (int)ST_TIMEOUT);
 }
 
+// ---------------------------------------------------------------------------
+// Persistent form of the same pass: one CTA per SM walks tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ...; the TMA / convert / MMA pipeline
+// runs on across tile boundaries, and two TMEM accumulators (2 x BN columns)
+// let the epilogue of one tile overlap the main loop of the next.  The
+// arithmetic of every tile (MMA order, epilogue) is that of k_dct_umma, so
+// the two kernels give identical results.
+//   warp 0      TMA producer         warp 1      TMEM owner, MMA issuer
+//   warps 2..5  converters           warps 6..9  epilogue (TMEM lanes 32*(warp%4))
+// ---------------------------------------------------------------------------
+constexpr int UMP_THREADS = 320;
+
+template <int BN>
+struct UmmaPSmem {
+    static constexpr uint32_t A_BYTES = UM_BM * UM_BK * 4;
+    static constexpr uint32_t B_BYTES = BN * UM_BK * 4;
+    static constexpr uint32_t STAGE = 2 * A_BYTES + 2 * B_BYTES;
+    static constexpr uint32_t EPI_OFF = UM_STAGES * STAGE;            // 4 x 32x33 floats
+    static constexpr uint32_t BAR_OFF = EPI_OFF + 4 * 32 * 33 * 4;
+    // full[2] conv[2] empty[2] tfull[2] tempty[2] done, TMEM address, abort
+    static constexpr uint32_t TOTAL = BAR_OFF + 128;
+    static constexpr uint32_t DYN = TOTAL + 1024;
+};
+
+template <int BN>
+__global__ void __launch_bounds__(UMP_THREADS, 1)
+    k_dct_umma_p(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmBh,
+                 const __grid_constant__ CUtensorMap tmBl, int K, int ntiles, UmmaEpi e, float* __restrict__ out,
+                 int* __restrict__ status)
+{
+    using L = UmmaPSmem<BN>;
+    extern __shared__ uint8_t ump_raw[];
+    uint8_t* sm = (uint8_t*)(((uintptr_t)ump_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* bars = (uint64_t*)(sm + L::BAR_OFF);
+    uint64_t* full = bars;
+    uint64_t* conv = bars + 2;
+    uint64_t* empty = bars + 4;
+    uint64_t* tfull = bars + 6;
+    uint64_t* tempty = bars + 8;
+    uint64_t* done = bars + 10;
+    volatile uint32_t* tmem_slot = (volatile uint32_t*)(bars + 11);
+    volatile int* abort_flag = (volatile int*)(bars + 12);
+    constexpr uint32_t TCOLS = 2 * BN;   // two accumulators
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nk = K / UM_BK;
+    // tiles of this CTA: blockIdx.x + it * gridDim.x, it < nmine
+    const int nmine = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < UM_STAGES; ++s) {
+            um_bar_init(&full[s], 1);
+            um_bar_init(&conv[s], 128);
+            um_bar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            um_bar_init(&tfull[a], 1);
+            um_bar_init(&tempty[a], 128);
+        }
+        um_bar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                         um_smem((const void*)tmem_slot)),
+                     "r"(TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const int total = nmine * nk;   // k-chunks this CTA streams
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int last[UM_STAGES] = {-1, -1};
+            for (int g = 0; g < total; ++g) {
+                const int s = g & 1, kc = g % nk;
+                const int m0 = ((int)blockIdx.x + (g / nk) * (int)gridDim.x) * UM_BM;
+                if (g >= UM_STAGES && !um_wait(&empty[s], ((g >> 1) + 1) & 1, abort_flag, true)) break;
+                uint8_t* st = sm + s * L::STAGE;
+                um_arrive_tx(&full[s], L::A_BYTES + 2 * L::B_BYTES);
+                um_tma_2d(st, &tmA, &full[s], kc * UM_BK, m0);
+                um_tma_2d(st + 2 * L::A_BYTES, &tmBh, &full[s], kc * UM_BK, 0);
+                um_tma_2d(st + 2 * L::A_BYTES + L::B_BYTES, &tmBl, &full[s], kc * UM_BK, 0);
+                last[s] = g;
+            }
+            for (int s = 0; s < UM_STAGES; ++s)
+                if (last[s] >= 0) um_wait(&full[s], (last[s] >> 1) & 1, abort_flag, false);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = um_idesc_tf32<BN>();
+            bool ok = true;
+            for (int it = 0; it < nmine && ok; ++it) {
+                const int a = it & 1;
+                if (it >= 2 && !um_wait(&tempty[a], ((it >> 1) + 1) & 1, abort_flag, true)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t acc = tmem + (uint32_t)(a * BN);
+                for (int kc = 0; kc < nk; ++kc) {
+                    const int g = it * nk + kc, s = g & 1;
+                    if (!um_wait(&conv[s], (g >> 1) & 1, abort_flag, true)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                    const uint32_t st = um_smem(sm + s * L::STAGE);
+                    const uint64_t dh = um_desc_sw128(st);
+                    const uint64_t dl = um_desc_sw128(st + L::A_BYTES);
+                    const uint64_t bh = um_desc_sw128(st + 2 * L::A_BYTES);
+                    const uint64_t bl = um_desc_sw128(st + 2 * L::A_BYTES + L::B_BYTES);
+#pragma unroll
+                    for (int kk = 0; kk < UM_BK / 8; ++kk) {
+                        const uint64_t o = (uint64_t)(kk * 32) >> 4;
+                        um_mma(acc, dl + o, bh + o, idesc, (kc | kk) ? 1u : 0u);
+                        um_mma(acc, dh + o, bl + o, idesc, 1u);
+                        um_mma(acc, dh + o, bh + o, idesc, 1u);
+                    }
+                    um_commit(&empty[s]);
+                }
+                if (ok) um_commit(&tfull[a]);
+            }
+            um_commit(done);   // tracks every MMA issued above
+        }
+        __syncwarp();
+    } else if (warp < 6) {
+        const int ct = threadIdx.x - 64;   // 0..127
+        for (int g = 0; g < total; ++g) {
+            const int s = g & 1;
+            if (!um_wait(&full[s], (g >> 1) & 1, abort_flag, true)) break;
+            float4* a = (float4*)(sm + s * L::STAGE);
+            float4* lo = (float4*)(sm + s * L::STAGE + L::A_BYTES);
+#pragma unroll 4
+            for (int i = ct; i < (int)(L::A_BYTES / 16); i += 128) {
+                float4 x = a[i], h, l;
+                h.x = um_rna_tf32(x.x); l.x = um_rna_tf32(x.x - h.x);
+                h.y = um_rna_tf32(x.y); l.y = um_rna_tf32(x.y - h.y);
+                h.z = um_rna_tf32(x.z); l.z = um_rna_tf32(x.z - h.z);
+                h.w = um_rna_tf32(x.w); l.w = um_rna_tf32(x.w - h.w);
+                a[i] = h;
+                lo[i] = l;
+            }
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            um_arrive(&conv[s]);
+        }
+    } else {
+        // epilogue warps 6..9: TMEM lane quadrant q = warp % 4
+        const int q = warp & 3;
+        float* buf = (float*)(sm + L::EPI_OFF) + (warp - 6) * 32 * 33;
+        for (int it = 0; it < nmine; ++it) {
+            const int a = it & 1;
+            if (!um_wait(&tfull[a], (it >> 1) & 1, abort_flag, true)) break;
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t trow = tmem + (uint32_t)(a * BN) + ((uint32_t)(32 * q) << 16);
+            const long m0 = ((long)blockIdx.x + (long)it * gridDim.x) * UM_BM;
+            if (e.transposed) {
+                const long r = m0 + 32 * q + lane;
+                float* o = out + (r / e.rows_per_plane) * e.ob + (r % e.rows_per_plane) * e.oq;
+                for (int c0 = 0; c0 < BN; c0 += 16) {
+                    uint32_t v[16];
+                    um_ld16(trow + c0, v);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        float x = __uint_as_float(v[j]);
+                        if (e.scale_mode == 1) x = x * e.scale;
+                        else if (e.scale_mode == 2) x = x / e.scale;
+                        o[(long)(c0 + j) * e.on] = x;
+                    }
+                }
+            } else {
+                for (int c0 = 0; c0 < BN; c0 += 32) {
+                    uint32_t v[32];
+                    um_ld16(trow + c0, v);
+                    um_ld16(trow + c0 + 16, v + 16);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) buf[lane * 33 + j] = __uint_as_float(v[j]);
+                    __syncwarp();
+                    for (int rr = 0; rr < 32; ++rr) {
+                        const long r = m0 + 32 * q + rr;
+                        float x = buf[rr * 33 + lane];
+                        if (e.scale_mode == 1) x = x * e.scale;
+                        else if (e.scale_mode == 2) x = x / e.scale;
+                        out[(r / e.rows_per_plane) * e.ob + (r % e.rows_per_plane) * e.oq + (long)(c0 + lane) * e.on] =
+                            x;
+                    }
+                    __syncwarp();
+                }
+            }
+            // this accumulator is read out: the MMA warp may overwrite it
+            asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+            um_arrive(&tempty[a]);
+        }
+    }
+
+    // every role: the MMAs issued (also after an abort) retire before TMEM goes
+    um_wait(done, 0, abort_flag, false);
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
+    }
+    if (threadIdx.x == 0 && *abort_flag) atomicOr(status, (int)ST_TIMEOUT);
+}
+
 }  // namespace
 }  // namespace pll

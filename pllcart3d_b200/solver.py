@@ -33,8 +33,9 @@ class Solver:
     """precision="fp64": the reference's FP64 arithmetic; "mixed": FP32 state
     and stencils, split-TF32 tensor-core DCT, FP64 Poisson mode solve and
     reductions.  dct_kernel="auto" runs the precision form's DCT passes as
-    tcgen05 GEMMs where the plane shape allows (ny, nz in {128, 256}),
-    "mma_sync" keeps the warp-level split-TF32 GEMM."""
+    tcgen05 GEMMs where the plane shape allows (ny, nz in {128, 256}; a
+    persistent kernel, one CTA per SM), "umma_tile" the same tcgen05 pass
+    with one tile per CTA, "mma_sync" the warp-level split-TF32 GEMM."""
 
     def __init__(self, params: Params, device: int = 0, exact_dct: bool = False,
                  use_graph: bool = True, precision: str = "fp64", dct_kernel: str = "auto"):
@@ -72,7 +73,7 @@ class Solver:
         p.precision = PRECISIONS[precision]
         p.exact_dct = int(bool(exact_dct))
         p.use_graph = int(bool(use_graph))
-        p.dct_kernel = {"auto": 0, "mma_sync": 1}[dct_kernel]
+        p.dct_kernel = {"auto": 0, "mma_sync": 1, "umma_tile": 2}[dct_kernel]
         return p
 
     # ---- lifetime ---------------------------------------------------------
