@@ -76,9 +76,20 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
     const int lb = tune_line_block(ctx->tune_line);
     k_line_pf<VAR, 1, real><<<dim3((nk(R) + lb - 1) / lb, ni(R)), lb, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
     mark(ctx, ly[VAR]);
-    constexpr size_t smem = adi_z_smem_bytes<VAR, real>();
-    k_adi_z_tiled<VAR, real><<<dim3((nj(R) + 127) / 128, ni(R)), 128, smem, ctx->st>>>(
-        ctx->G, R, ctx->K, X.mu, B.S, B.cc, ctx->scal, alpha);
+    bool zdone = false;
+    if constexpr (std::is_same<real, float>::value) {
+        if (nk(R) <= ZP_MAX && nk(R) >= 2 * (ZP_MAX / 32) && !ctx->P.exact_dct) {
+            // the precision form's partitioned warp solve
+            k_adi_z_part<VAR><<<dim3((nj(R) + 3) / 4, ni(R)), 128, 0, ctx->st>>>(ctx->G, R, ctx->K, X.mu, B.S,
+                                                                               ctx->scal, alpha);
+            zdone = true;
+        }
+    }
+    if (!zdone) {
+        constexpr size_t smem = adi_z_smem_bytes<VAR, real>();
+        k_adi_z_tiled<VAR, real><<<dim3((nj(R) + 127) / 128, ni(R)), 128, smem, ctx->st>>>(
+            ctx->G, R, ctx->K, X.mu, B.S, B.cc, ctx->scal, alpha);
+    }
     mark(ctx, lz[VAR]);
     k_line_pf<VAR, 0, real><<<dim3((nk(R) + lb - 1) / lb, nj(R)), lb, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
     mark(ctx, lx[VAR]);

@@ -752,6 +752,172 @@ __global__ void __launch_bounds__(128, 4) k_adi_z_tiled(Geo G, Rng R, Consts K, 
 
 
 // ---------------------------------------------------------------------------
+// The precision form's z line solve: one warp per line, the line held in
+// registers (8 rows per lane) and solved by a partition method instead of
+// the sequential Thomas chain.  Row 8l of each lane is a separator; the lane
+// eliminates its 7 interior rows in terms of its own separator and the next
+// lane's (x_e = g_e - v_e S_l - w_e S_{l+1}), the 32 separator equations
+// form a tridiagonal system solved by parallel cyclic reduction over warp
+// shuffles, and the interior rows follow.  S is read once and the solution
+// written once (the Thomas form also writes and re-reads c' and the
+// eliminated right-hand side).  Same coefficients and closures as
+// k_adi_z_tiled; FP32-level agreement, not bitwise.  Lines of up to 256.
+// Rows move between global memory (coalesced, row m by lane m % 32) and the
+// lane that owns them (8l .. 8l+7) through a skewed shared buffer.
+// ---------------------------------------------------------------------------
+constexpr int ZP_MAX = 256;
+__device__ __forceinline__ int zp_skew(int m) { return m + (m >> 3); }
+
+template <int VAR>
+__global__ void __launch_bounds__(128) k_adi_z_part(Geo G, Rng R, Consts K, MuPtrs<float> mu,
+                                                    float* __restrict__ S, const double* __restrict__ scal,
+                                                    double alpha)
+{
+    constexpr int E = ZP_MAX / 32;   // rows per lane
+    constexpr int BUF = ZP_MAX + ZP_MAX / 8 + 8;
+    __shared__ float bS[4][BUF];
+    __shared__ float bM[4][BUF];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int j = R.js + blockIdx.x * 4 + warp;
+    const int i = R.is + blockIdx.y;
+    if (j > R.je) return;   // warp-uniform
+    const int n = R.ke - R.ks + 1;
+    const float fac = (float)(0.5 * scal[S_DT] * alpha);
+    constexpr int LO = Closure<VAR, 2>::lo, HI = Closure<VAR, 2>::hi;
+    const float* __restrict__ mz = VAR == VU ? mu.xz : VAR == VV ? mu.yz : mu.cell;
+    const int moff = VAR == VW ? -1 : 0;
+    const float dzc = (float)(VAR == VW ? K.d2z : K.d1z);
+    const float ihz = (float)K.ihz, cdz = (float)K.cdz;
+    const long base = (long)i * G.sx + (long)j * G.sy + R.ks;
+    float* sS = bS[warp];
+    float* sM = bM[warp];
+#pragma unroll
+    for (int t = 0; t < E; ++t) {
+        const int m = t * 32 + lane;
+        if (m < n) sS[zp_skew(m)] = S[base + m];
+        if (VAR != VC && m <= n) sM[zp_skew(m)] = mz[base + moff + m];
+    }
+    if (VAR != VC && lane == 0 && n == ZP_MAX) sM[zp_skew(ZP_MAX)] = mz[base + moff + ZP_MAX];
+    __syncwarp();
+
+    // this lane's rows m = 8 lane + e: a x_{m-1} + b x_m + c x_{m+1} = r
+    float A[E], B[E], C[E], Rr[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int m = E * lane + e;
+        if (m < n) {
+            float a, c;
+            if (VAR == VC) {
+                a = cdz;
+                c = cdz;
+            } else {
+                a = dzc * sM[zp_skew(m)] * ihz;
+                c = dzc * sM[zp_skew(m + 1)] * ihz;
+            }
+            const float b = -(a + c);
+            float la = -fac * a, lb = 1.0f - fac * b, lc = -fac * c, lr = sS[zp_skew(m)];
+            if (m == 0) {
+                if (LO == 1) lb += la;
+                else if (LO == 2) lb -= la;
+                la = 0.f;
+            }
+            if (m == n - 1) {
+                if (HI == 1) lb += lc;
+                else if (HI == 2) lb -= lc;
+                lc = 0.f;
+            }
+            A[e] = la;
+            B[e] = lb;
+            C[e] = lc;
+            Rr[e] = lr;
+        } else {   // identity rows past the line
+            A[e] = 0.f;
+            B[e] = 1.f;
+            C[e] = 0.f;
+            Rr[e] = 0.f;
+        }
+    }
+    // interior rows e = 1..E-1: forward in terms of the own separator S_l
+    float ch[E], rh[E], ah[E];
+    {
+        const float ib = __fdividef(1.0f, B[1]);
+        ch[1] = C[1] * ib;
+        rh[1] = Rr[1] * ib;
+        ah[1] = A[1] * ib;
+    }
+#pragma unroll
+    for (int e = 2; e < E; ++e) {
+        const float id = __fdividef(1.0f, B[e] - A[e] * ch[e - 1]);
+        ch[e] = C[e] * id;
+        rh[e] = (Rr[e] - A[e] * rh[e - 1]) * id;
+        ah[e] = -A[e] * ah[e - 1] * id;
+    }
+    // backward: x_e = g_e - v_e S_l - w_e S_{l+1}
+    float g[E], v[E], w[E];
+    g[E - 1] = rh[E - 1];
+    v[E - 1] = ah[E - 1];
+    w[E - 1] = ch[E - 1];
+#pragma unroll
+    for (int e = E - 2; e >= 1; --e) {
+        g[e] = rh[e] - ch[e] * g[e + 1];
+        v[e] = ah[e] - ch[e] * v[e + 1];
+        w[e] = -ch[e] * w[e + 1];
+    }
+    // separator row 8l: A0 x_{8l-1} + B0 S_l + C0 x_{8l+1} = R0
+    float gp = __shfl_up_sync(0xffffffffu, g[E - 1], 1);
+    float vp = __shfl_up_sync(0xffffffffu, v[E - 1], 1);
+    float wp = __shfl_up_sync(0xffffffffu, w[E - 1], 1);
+    if (lane == 0) gp = vp = wp = 0.f;
+    float al = -A[0] * vp;
+    float be = B[0] - A[0] * wp - C[0] * v[1];
+    float ga = -C[0] * w[1];
+    float rho = Rr[0] - A[0] * gp - C[0] * g[1];
+    // parallel cyclic reduction of the 32 separator equations
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        float al_m = __shfl_up_sync(0xffffffffu, al, d), be_m = __shfl_up_sync(0xffffffffu, be, d);
+        float ga_m = __shfl_up_sync(0xffffffffu, ga, d), rho_m = __shfl_up_sync(0xffffffffu, rho, d);
+        float al_p = __shfl_down_sync(0xffffffffu, al, d), be_p = __shfl_down_sync(0xffffffffu, be, d);
+        float ga_p = __shfl_down_sync(0xffffffffu, ga, d), rho_p = __shfl_down_sync(0xffffffffu, rho, d);
+        if (lane < d) {
+            al_m = 0.f;
+            be_m = 1.f;
+            ga_m = 0.f;
+            rho_m = 0.f;
+        }
+        if (lane + d > 31) {
+            al_p = 0.f;
+            be_p = 1.f;
+            ga_p = 0.f;
+            rho_p = 0.f;
+        }
+        const float k1 = __fdividef(al, be_m), k2 = __fdividef(ga, be_p);
+        const float nal = -k1 * al_m, nga = -k2 * ga_p;
+        be = be - k1 * ga_m - k2 * al_p;
+        rho = rho - k1 * rho_m - k2 * rho_p;
+        al = nal;
+        ga = nga;
+    }
+    const float Sl = __fdividef(rho, be);
+    float Sn = __shfl_down_sync(0xffffffffu, Sl, 1);
+    if (lane == 31) Sn = 0.f;
+    float x[E];
+    x[0] = Sl;
+#pragma unroll
+    for (int e = 1; e < E; ++e) x[e] = g[e] - v[e] * Sl - w[e] * Sn;
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < E; ++e) sS[zp_skew(E * lane + e)] = x[e];
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < E; ++t) {
+        const int m = t * 32 + lane;
+        if (m < n) S[base + m] = sS[zp_skew(m)];
+    }
+}
+
+
+// ---------------------------------------------------------------------------
 // Viscosity family and offset that the implicit coefficients of VAR along
 // AXIS read (A_umom/A_vmom/A_wmom, pllcart3d.c:1443-1536): a at line
 // position m uses family[m + OFF], c uses family[m + OFF + 1]; the scale is
