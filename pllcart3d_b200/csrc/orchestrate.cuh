@@ -74,7 +74,18 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
     X.r = r;
     X.alpha = alpha;
     const int lb = tune_line_block(ctx->tune_line);
-    k_line_pf<VAR, 1, real><<<dim3((nk(R) + lb - 1) / lb, ni(R)), lb, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
+    bool ydone = false;
+    if constexpr (std::is_same<real, float>::value) {
+        // the precision form's partitioned warp solve; for momentum the
+        // prefetching Thomas sweep measures faster and stays
+        if (VAR == VC && nj(R) <= ZP_MAX && nj(R) >= 2 * (ZP_MAX / 32) && !ctx->P.exact_dct) {
+            k_adi_y_part<VAR><<<dim3((nk(R) + 31) / 32, ni(R)), 256, adi_y_part_smem(), ctx->st>>>(
+                ctx->G, R, ctx->K, X.mu, B.S, ctx->scal, alpha);
+            ydone = true;
+        }
+    }
+    if (!ydone)
+        k_line_pf<VAR, 1, real><<<dim3((nk(R) + lb - 1) / lb, ni(R)), lb, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
     mark(ctx, ly[VAR]);
     bool zdone = false;
     if constexpr (std::is_same<real, float>::value) {
@@ -676,6 +687,12 @@ bool alloc_state(pllgpu_ctx* c)
     dct_matrix<real>(1, p->nz, T.data());
     cudaMemcpy(B.Tiz, T.data(), sizeof(real) * p->nz * p->nz, cudaMemcpyHostToDevice);
     // kernels above the 48 KB default of dynamic shared memory
+    if constexpr (std::is_same<real, float>::value) {
+        cudaFuncSetAttribute(k_adi_y_part<VC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adi_y_part_smem());
+        cudaFuncSetAttribute(k_adi_y_part<VU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adi_y_part_smem());
+        cudaFuncSetAttribute(k_adi_y_part<VV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adi_y_part_smem());
+        cudaFuncSetAttribute(k_adi_y_part<VW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adi_y_part_smem());
+    }
     cudaFuncSetAttribute(k_adi_z_tiled<VC, real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)adi_z_smem_bytes<VC, real>());
     cudaFuncSetAttribute(k_adi_z_tiled<VU, real>, cudaFuncAttributeMaxDynamicSharedMemorySize,

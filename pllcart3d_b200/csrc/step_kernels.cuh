@@ -768,6 +768,86 @@ __global__ void __launch_bounds__(128, 4) k_adi_z_tiled(Geo G, Rng R, Consts K, 
 constexpr int ZP_MAX = 256;
 __device__ __forceinline__ int zp_skew(int m) { return m + (m >> 3); }
 
+// Partitioned solve of one line of 32 E rows held E per lane (rows
+// E l .. E l + E - 1 on lane l; a of the first row and c of the last are 0;
+// rows past the line are identity rows): row E l of each lane is a
+// separator, the lane eliminates its E-1 interior rows in terms of its own
+// separator and the next lane's (x_e = g_e - v_e S_l - w_e S_{l+1}), the 32
+// separator equations are solved by parallel cyclic reduction over warp
+// shuffles, then the interior rows.  FP32, diagonally dominant systems.
+template <int E>
+__device__ __forceinline__ void zp_solve(const float* A, const float* B, const float* C, const float* Rr, float* x,
+                                         int lane)
+{
+    // interior rows e = 1..E-1: forward in terms of the own separator S_l
+    float ch[E], rh[E], ah[E];
+    {
+        const float ib = __fdividef(1.0f, B[1]);
+        ch[1] = C[1] * ib;
+        rh[1] = Rr[1] * ib;
+        ah[1] = A[1] * ib;
+    }
+#pragma unroll
+    for (int e = 2; e < E; ++e) {
+        const float id = __fdividef(1.0f, B[e] - A[e] * ch[e - 1]);
+        ch[e] = C[e] * id;
+        rh[e] = (Rr[e] - A[e] * rh[e - 1]) * id;
+        ah[e] = -A[e] * ah[e - 1] * id;
+    }
+    // backward: x_e = g_e - v_e S_l - w_e S_{l+1}
+    float g[E], v[E], w[E];
+    g[E - 1] = rh[E - 1];
+    v[E - 1] = ah[E - 1];
+    w[E - 1] = ch[E - 1];
+#pragma unroll
+    for (int e = E - 2; e >= 1; --e) {
+        g[e] = rh[e] - ch[e] * g[e + 1];
+        v[e] = ah[e] - ch[e] * v[e + 1];
+        w[e] = -ch[e] * w[e + 1];
+    }
+    // separator row 8l: A0 x_{8l-1} + B0 S_l + C0 x_{8l+1} = R0
+    float gp = __shfl_up_sync(0xffffffffu, g[E - 1], 1);
+    float vp = __shfl_up_sync(0xffffffffu, v[E - 1], 1);
+    float wp = __shfl_up_sync(0xffffffffu, w[E - 1], 1);
+    if (lane == 0) gp = vp = wp = 0.f;
+    float al = -A[0] * vp;
+    float be = B[0] - A[0] * wp - C[0] * v[1];
+    float ga = -C[0] * w[1];
+    float rho = Rr[0] - A[0] * gp - C[0] * g[1];
+    // parallel cyclic reduction of the 32 separator equations
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        float al_m = __shfl_up_sync(0xffffffffu, al, d), be_m = __shfl_up_sync(0xffffffffu, be, d);
+        float ga_m = __shfl_up_sync(0xffffffffu, ga, d), rho_m = __shfl_up_sync(0xffffffffu, rho, d);
+        float al_p = __shfl_down_sync(0xffffffffu, al, d), be_p = __shfl_down_sync(0xffffffffu, be, d);
+        float ga_p = __shfl_down_sync(0xffffffffu, ga, d), rho_p = __shfl_down_sync(0xffffffffu, rho, d);
+        if (lane < d) {
+            al_m = 0.f;
+            be_m = 1.f;
+            ga_m = 0.f;
+            rho_m = 0.f;
+        }
+        if (lane + d > 31) {
+            al_p = 0.f;
+            be_p = 1.f;
+            ga_p = 0.f;
+            rho_p = 0.f;
+        }
+        const float k1 = __fdividef(al, be_m), k2 = __fdividef(ga, be_p);
+        const float nal = -k1 * al_m, nga = -k2 * ga_p;
+        be = be - k1 * ga_m - k2 * al_p;
+        rho = rho - k1 * rho_m - k2 * rho_p;
+        al = nal;
+        ga = nga;
+    }
+    const float Sl = __fdividef(rho, be);
+    float Sn = __shfl_down_sync(0xffffffffu, Sl, 1);
+    if (lane == 31) Sn = 0.f;
+    x[0] = Sl;
+#pragma unroll
+    for (int e = 1; e < E; ++e) x[e] = g[e] - v[e] * Sl - w[e] * Sn;
+}
+
 template <int VAR>
 __global__ void __launch_bounds__(128) k_adi_z_part(Geo G, Rng R, Consts K, MuPtrs<float> mu,
                                                     float* __restrict__ S, const double* __restrict__ scal,
@@ -837,74 +917,8 @@ __global__ void __launch_bounds__(128) k_adi_z_part(Geo G, Rng R, Consts K, MuPt
             Rr[e] = 0.f;
         }
     }
-    // interior rows e = 1..E-1: forward in terms of the own separator S_l
-    float ch[E], rh[E], ah[E];
-    {
-        const float ib = __fdividef(1.0f, B[1]);
-        ch[1] = C[1] * ib;
-        rh[1] = Rr[1] * ib;
-        ah[1] = A[1] * ib;
-    }
-#pragma unroll
-    for (int e = 2; e < E; ++e) {
-        const float id = __fdividef(1.0f, B[e] - A[e] * ch[e - 1]);
-        ch[e] = C[e] * id;
-        rh[e] = (Rr[e] - A[e] * rh[e - 1]) * id;
-        ah[e] = -A[e] * ah[e - 1] * id;
-    }
-    // backward: x_e = g_e - v_e S_l - w_e S_{l+1}
-    float g[E], v[E], w[E];
-    g[E - 1] = rh[E - 1];
-    v[E - 1] = ah[E - 1];
-    w[E - 1] = ch[E - 1];
-#pragma unroll
-    for (int e = E - 2; e >= 1; --e) {
-        g[e] = rh[e] - ch[e] * g[e + 1];
-        v[e] = ah[e] - ch[e] * v[e + 1];
-        w[e] = -ch[e] * w[e + 1];
-    }
-    // separator row 8l: A0 x_{8l-1} + B0 S_l + C0 x_{8l+1} = R0
-    float gp = __shfl_up_sync(0xffffffffu, g[E - 1], 1);
-    float vp = __shfl_up_sync(0xffffffffu, v[E - 1], 1);
-    float wp = __shfl_up_sync(0xffffffffu, w[E - 1], 1);
-    if (lane == 0) gp = vp = wp = 0.f;
-    float al = -A[0] * vp;
-    float be = B[0] - A[0] * wp - C[0] * v[1];
-    float ga = -C[0] * w[1];
-    float rho = Rr[0] - A[0] * gp - C[0] * g[1];
-    // parallel cyclic reduction of the 32 separator equations
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        float al_m = __shfl_up_sync(0xffffffffu, al, d), be_m = __shfl_up_sync(0xffffffffu, be, d);
-        float ga_m = __shfl_up_sync(0xffffffffu, ga, d), rho_m = __shfl_up_sync(0xffffffffu, rho, d);
-        float al_p = __shfl_down_sync(0xffffffffu, al, d), be_p = __shfl_down_sync(0xffffffffu, be, d);
-        float ga_p = __shfl_down_sync(0xffffffffu, ga, d), rho_p = __shfl_down_sync(0xffffffffu, rho, d);
-        if (lane < d) {
-            al_m = 0.f;
-            be_m = 1.f;
-            ga_m = 0.f;
-            rho_m = 0.f;
-        }
-        if (lane + d > 31) {
-            al_p = 0.f;
-            be_p = 1.f;
-            ga_p = 0.f;
-            rho_p = 0.f;
-        }
-        const float k1 = __fdividef(al, be_m), k2 = __fdividef(ga, be_p);
-        const float nal = -k1 * al_m, nga = -k2 * ga_p;
-        be = be - k1 * ga_m - k2 * al_p;
-        rho = rho - k1 * rho_m - k2 * rho_p;
-        al = nal;
-        ga = nga;
-    }
-    const float Sl = __fdividef(rho, be);
-    float Sn = __shfl_down_sync(0xffffffffu, Sl, 1);
-    if (lane == 31) Sn = 0.f;
     float x[E];
-    x[0] = Sl;
-#pragma unroll
-    for (int e = 1; e < E; ++e) x[e] = g[e] - v[e] * Sl - w[e] * Sn;
+    zp_solve<E>(A, B, C, Rr, x, lane);
     __syncwarp();
 #pragma unroll
     for (int e = 0; e < E; ++e) sS[zp_skew(E * lane + e)] = x[e];
@@ -955,6 +969,104 @@ __device__ __forceinline__ void line_ac(const Consts& K, real m0, real m1, real&
                                                      : (AXIS == 0 ? K.d1x : AXIS == 1 ? K.d1y : K.d1z);
         a = over_h<real>((real)d * m0, h, ih, K.pow2);
         c = over_h<real>((real)d * m1, h, ih, K.pow2);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The precision form's y line solve with the same partitioned warp solver:
+// a block of 8 warps stages 32 neighbouring lines (consecutive k, coalesced
+// rows of the tile) and their viscosity family through shared memory, each
+// warp solves 4 of them, the block writes the solutions back in place.  Same
+// coefficients and closures as k_line_pf<VAR, 1>; S read once, written once.
+// ---------------------------------------------------------------------------
+constexpr int YP_PITCH = ZP_MAX + ZP_MAX / 8 + 1;   // odd: conflict-free columns
+
+constexpr size_t adi_y_part_smem() { return sizeof(float) * 2 * 32 * YP_PITCH; }
+
+template <int VAR>
+__global__ void __launch_bounds__(256) k_adi_y_part(Geo G, Rng R, Consts K, MuPtrs<float> mu,
+                                                    float* __restrict__ S, const double* __restrict__ scal,
+                                                    double alpha)
+{
+    constexpr int E = ZP_MAX / 32;
+    extern __shared__ float ysm[];
+    float* tS = ysm;                      // [32 lines][YP_PITCH]
+    float* tM = ysm + 32 * YP_PITCH;
+    const int i = R.is + blockIdx.y;
+    const int k0 = R.ks + blockIdx.x * 32;
+    const int nl = (R.ke - k0 + 1) < 32 ? (R.ke - k0 + 1) : 32;
+    const int n = R.je - R.js + 1;
+    const long sy = G.sy;
+    const long base0 = (long)i * G.sx + (long)R.js * sy + k0;
+    constexpr int OFF = LineCoef<VAR, 1>::off;
+    const float* __restrict__ fam = VAR == VC ? nullptr : line_family<VAR, 1, float>(mu);
+    const float dy = (float)(LineCoef<VAR, 1>::twice ? K.d2y : K.d1y);
+    const float ihy = (float)K.ihy, cdy = (float)K.cdy;
+    const float fac = (float)(0.5 * scal[S_DT] * alpha);
+    constexpr int LO = Closure<VAR, 1>::lo, HI = Closure<VAR, 1>::hi;
+    // tile loads: thread (kl, row group m0) moves rows m0, m0 + 8, ...;
+    // unrolled so that many rows' loads are in flight at once
+    const int tkl = threadIdx.x & 31, tm0 = threadIdx.x >> 5;
+#pragma unroll 11
+    for (int t = 0; t < ZP_MAX / 8 + 1; ++t) {
+        const int m = tm0 + 8 * t;
+        if (tkl < nl && m <= n) {
+            if (m < n) tS[tkl * YP_PITCH + zp_skew(m)] = S[base0 + (long)m * sy + tkl];
+            if (VAR != VC) tM[tkl * YP_PITCH + zp_skew(m)] = fam[base0 + (long)(m + OFF) * sy + tkl];
+        }
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int kl = warp; kl < nl; kl += 8) {
+        const float* ls = tS + kl * YP_PITCH;
+        const float* lm = tM + kl * YP_PITCH;
+        float A[E], B[E], C[E], Rr[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int m = E * lane + e;
+            if (m < n) {
+                float a, c;
+                if (VAR == VC) {
+                    a = cdy;
+                    c = cdy;
+                } else {
+                    a = dy * lm[zp_skew(m)] * ihy;
+                    c = dy * lm[zp_skew(m + 1)] * ihy;
+                }
+                const float b = -(a + c);
+                float la = -fac * a, lb = 1.0f - fac * b, lc = -fac * c;
+                if (m == 0) {
+                    if (LO == 1) lb += la;
+                    else if (LO == 2) lb -= la;
+                    la = 0.f;
+                }
+                if (m == n - 1) {
+                    if (HI == 1) lb += lc;
+                    else if (HI == 2) lb -= lc;
+                    lc = 0.f;
+                }
+                A[e] = la;
+                B[e] = lb;
+                C[e] = lc;
+                Rr[e] = ls[zp_skew(m)];
+            } else {
+                A[e] = 0.f;
+                B[e] = 1.f;
+                C[e] = 0.f;
+                Rr[e] = 0.f;
+            }
+        }
+        float x[E];
+        zp_solve<E>(A, B, C, Rr, x, lane);
+        __syncwarp();
+#pragma unroll
+        for (int e = 0; e < E; ++e) tS[kl * YP_PITCH + zp_skew(E * lane + e)] = x[e];
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int t = 0; t < ZP_MAX / 8; ++t) {
+        const int m = tm0 + 8 * t;
+        if (tkl < nl && m < n) S[base0 + (long)m * sy + tkl] = tS[tkl * YP_PITCH + zp_skew(m)];
     }
 }
 
