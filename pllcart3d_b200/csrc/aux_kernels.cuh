@@ -31,9 +31,15 @@ __device__ __forceinline__ real visc_law(real cavg, const Consts& K, int nmvp,
     return (real)(scal[S_MUM] * sin(psi));
 }
 
+// planes of i one k_viscosity thread walks
+constexpr int VISC_NI = 4;
+
 // calculate_viscosity (pllcart3d.c:843-886): mu at cell centres on the box
 // padded by one cell, and on the xy / xz / yz edge families.  One thread per
-// (i,j,k) of i in [is-1, ie+1], j in [0, NY-1], k in [0, NZ-1].
+// (j,k) of j in [0, NY-1], k in [0, NZ-1], walking VISC_NI planes of i in
+// [is-1, ie+1]; the c values of plane i-1 that the xy and xz edges average
+// come from the previous plane's registers.  Every point read lies inside the
+// padded box's allocation (i >= is-1 >= 2), whether or not its value is used.
 template <typename real>
 __global__ void __launch_bounds__(128) k_viscosity(Geo G, Rng R, Consts K, int nmvp,
                                                    const real* __restrict__ cn, real* __restrict__ mc,
@@ -42,21 +48,29 @@ __global__ void __launch_bounds__(128) k_viscosity(Geo G, Rng R, Consts K, int n
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = R.is - 1 + blockIdx.z;
     if (k >= G.NZ || j >= G.NY) return;
-    const long sx = G.sx, sy = G.sy;
-    const long id = (long)i * sx + (long)j * sy + k;
-    mc[id] = visc_law<real>(cn[id], K, nmvp, scal);
-    const bool in_i = (i >= R.is), in_i2 = (i <= R.ie);
+    const int sx = (int)G.sx, sy = (int)G.sy;
+    const int i0 = R.is - 1 + blockIdx.z * VISC_NI;
     const bool jxy = (j >= R.js) & (j <= R.je + 1), jin = (j >= R.js) & (j <= R.je);
     const bool kin = (k >= R.ks) & (k <= R.ke), kxz = (k >= R.ks) & (k <= R.ke + 1);
     const real q = (real)0.25;
-    if (in_i & jxy & kin)
-        mxy[id] = visc_law<real>(q * (cn[id - sx - sy] + cn[id - sy] + cn[id - sx] + cn[id]), K, nmvp, scal);
-    if (in_i & jin & kxz)
-        mxz[id] = visc_law<real>(q * (cn[id - sx - 1] + cn[id - 1] + cn[id - sx] + cn[id]), K, nmvp, scal);
-    if (in_i & in_i2 & jxy & kxz)
-        myz[id] = visc_law<real>(q * (cn[id - sy - 1] + cn[id - 1] + cn[id - sy] + cn[id]), K, nmvp, scal);
+    int id = i0 * sx + j * sy + k;
+    // c at (i-1, j, k), (i-1, j-1, k), (i-1, j, k-1)
+    real p0 = cn[id - sx], py = cn[id - sx - sy], pz = cn[id - sx - 1];
+#pragma unroll
+    for (int t = 0; t < VISC_NI; ++t, id += sx) {
+        const int i = i0 + t;
+        if (i > R.ie + 1) break;
+        const real c0 = cn[id], cy = cn[id - sy], cz = cn[id - 1], cyz = cn[id - sy - 1];
+        mc[id] = visc_law<real>(c0, K, nmvp, scal);
+        const bool in_i = (i >= R.is), in_i2 = (i <= R.ie);
+        if (in_i & jxy & kin) mxy[id] = visc_law<real>(q * (py + cy + p0 + c0), K, nmvp, scal);
+        if (in_i & jin & kxz) mxz[id] = visc_law<real>(q * (pz + cz + p0 + c0), K, nmvp, scal);
+        if (in_i & in_i2 & jxy & kxz) myz[id] = visc_law<real>(q * (cyz + cz + cy + c0), K, nmvp, scal);
+        p0 = c0;
+        py = cy;
+        pz = cz;
+    }
 }
 
 // find_cfl (pllcart3d.c:3095-3118): max over interior cells of
@@ -351,117 +365,106 @@ __global__ void k_phi_ghosts(Geo G, Rng R, real* __restrict__ p)
     }
 }
 
-template <typename real>
-struct ProjectArgs {
-    real* u;
-    real* v;
-    real* w;               // new velocities, corrected in place
-    real* pgu;
-    real* pgv;
-    real* pgw;             // accumulated pressure gradients
-    const real* phi;
-    MuPtrs<real> mu;       // mu_new
-    const double* scal;    // dt, deficit
-    double alpha;
-    int do_correct, do_ghosts, do_pg;
-};
+// planes of i one k_project thread walks
+constexpr int PROJECT_NI = 1;
+
+// accumulated pressure gradient pold of component VAR at id advanced by
+// grad(phi) along its axis and the viscous operator applied to that gradient
+template <int VAR, typename real>
+__device__ __forceinline__ real pg_update(const Consts& K, const Geo& G, const real* __restrict__ phi,
+                                          const real* __restrict__ mc, const real* __restrict__ mxy,
+                                          const real* __restrict__ mxz, const real* __restrict__ myz,
+                                          int id, int sx, int sy, real fac, real pold)
+{
+    const int so = VAR == VU ? sx : VAR == VV ? sy : 1;
+    const double h = VAR == VU ? K.hx : VAR == VV ? K.hy : K.hz;
+    const double ih = VAR == VU ? K.ihx : VAR == VV ? K.ihy : K.ihz;
+    auto gp = [&](int p) { return over_h<real>(phi[p] - phi[p - so], h, ih, K.pow2); };
+    real a, b, c;
+    const real g0 = gp(id);
+    acoef<VAR, 0, real>(K, G, mc, mxy, mxz, myz, id, a, b, c);
+    const real pxx = a * gp(id - sx) + b * g0 + c * gp(id + sx);
+    acoef<VAR, 1, real>(K, G, mc, mxy, mxz, myz, id, a, b, c);
+    const real pyy = a * gp(id - sy) + b * g0 + c * gp(id + sy);
+    acoef<VAR, 2, real>(K, G, mc, mxy, mxz, myz, id, a, b, c);
+    const real pzz = a * gp(id - 1) + b * g0 + c * gp(id + 1);
+    return pold + g0 - fac * (pyy + pxx + pzz);
+}
 
 // velo_correction (pllcart3d.c:2133-2227), update_veloghost_points
 // (L2810-2885) and pressure_gradient (L2964-3044) fused: one thread per
-// (i,j,k) of i in [is, ie+1], j in [js, je], k in [ks, ke] of the grid.
-// Ghost copies are written by the thread that owns their source value, after
-// its correction.  grad(phi) at neighbours is evaluated from phi directly
-// (the reference's phi_x/phi_y/phi_z temporaries hold exactly these values).
+// (j,k) of j in [js, je], k in [ks, ke], walking PROJECT_NI planes of i in
+// [is, ie+1].  Ghost copies are written by the thread that owns their source
+// value, after its correction.  grad(phi) at neighbours is evaluated from phi
+// directly (the reference's phi_x/phi_y/phi_z temporaries hold exactly these
+// values).  Every pointer is a restrict-qualified parameter: the outputs
+// (u, v, w, pg) are written only at points no thread of the launch reads
+// (a thread's own u, v, w and ghosts outside the walked range), so the loads
+// of both planes may all be in flight before the first store.
 template <typename real>
 __global__ void __launch_bounds__(128) k_project(Geo G, Rng Rg, Rng Ru, Rng Rv, Rng Rw, Consts K,
-                                                 ProjectArgs<real> A)
+        real* __restrict__ u, real* __restrict__ v, real* __restrict__ w,
+        real* __restrict__ pgu, real* __restrict__ pgv, real* __restrict__ pgw,
+        const real* __restrict__ phi, const real* __restrict__ mc, const real* __restrict__ mxy,
+        const real* __restrict__ mxz, const real* __restrict__ myz, const double* __restrict__ scal,
+        double alpha, int do_correct, int do_ghosts, int do_pg)
 {
     const int k = Rg.ks + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = Rg.js + blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = Rg.is + blockIdx.z;
     if (k > Rg.ke || j > Rg.je) return;
-    const long sx = G.sx, sy = G.sy;
-    const long id = (long)i * sx + (long)j * sy + k;
-    const real* __restrict__ phi = A.phi;
-    const double dt = A.scal[S_DT];
-    const bool inu = (i >= Ru.is) & (i <= Ru.ie) & (j >= Ru.js) & (k >= Ru.ks);
-    const bool inv = (i <= Rv.ie) & (j >= Rv.js) & (k >= Rv.ks);
-    const bool inw = (i <= Rw.ie) & (j >= Rw.js) & (k >= Rw.ks);
-    const bool ghost_i = (i <= Rg.ie);
+    const int sx = (int)G.sx, sy = (int)G.sy;
+    const double dt = scal[S_DT];
+    const real cfac = (real)(dt * alpha / K.Re);
+    const real pfac = (real)(0.5 * dt * alpha);
+#pragma unroll
+    for (int t = 0; t < PROJECT_NI; ++t) {
+        const int i = Rg.is + blockIdx.z * PROJECT_NI + t;
+        if (i > Rg.ie + 1) break;
+        const int id = i * sx + j * sy + k;
+        const bool inu = (i >= Ru.is) & (i <= Ru.ie) & (j >= Ru.js) & (k >= Ru.ks);
+        const bool inv = (i <= Rv.ie) & (j >= Rv.js) & (k >= Rv.ks);
+        const bool inw = (i <= Rw.ie) & (j >= Rw.js) & (k >= Rw.ks);
+        const bool ghost_i = (i <= Rg.ie);
 
-    if (A.do_correct) {
-        const real fac = (real)(dt * A.alpha / K.Re);
-        real uval = A.u[id], vval = 0, wval = 0;
-        if (ghost_i) {
-            vval = A.v[id];
-            wval = A.w[id];
+        if (do_correct) {
+            real uval = u[id], vval = 0, wval = 0;
+            if (ghost_i) {
+                vval = v[id];
+                wval = w[id];
+            }
+            if (inv) {
+                vval = vval - cfac * over_h<real>(phi[id] - phi[id - sy], K.hy, K.ihy, K.pow2);
+                v[id] = vval;
+            }
+            if (inw) {
+                wval = wval - cfac * over_h<real>(phi[id] - phi[id - 1], K.hz, K.ihz, K.pow2);
+                w[id] = wval;
+            }
+            if (inu) {
+                uval = uval - cfac * over_h<real>(phi[id] - phi[id - sx], K.hx, K.ihx, K.pow2);
+                u[id] = uval;
+            }
+            if (i == Ru.ie + 1 && j >= Ru.js && k >= Ru.ks) u[id] = uval + (real)scal[S_DEFICIT];
+            if (do_ghosts && ghost_i) {
+                if (k == Rg.ks) { u[id - 1] = uval; v[id - 1] = vval; }
+                if (k == Rg.ke) { u[id + 1] = uval; v[id + 1] = vval; }
+                if (j == Rg.js) { u[id - sy] = -uval; w[id - sy] = -wval; }
+                if (j == Rg.je) { u[id + sy] = -uval; w[id + sy] = -wval; }
+                if (i == Rg.is) { v[id - sx] = -vval; w[id - sx] = -wval; }
+            }
+        } else if (do_ghosts && ghost_i) {
+            const real uval = u[id], vval = v[id], wval = w[id];
+            if (k == Rg.ks) { u[id - 1] = uval; v[id - 1] = vval; }
+            if (k == Rg.ke) { u[id + 1] = uval; v[id + 1] = vval; }
+            if (j == Rg.js) { u[id - sy] = -uval; w[id - sy] = -wval; }
+            if (j == Rg.je) { u[id + sy] = -uval; w[id + sy] = -wval; }
+            if (i == Rg.is) { v[id - sx] = -vval; w[id - sx] = -wval; }
         }
-        if (inv) {
-            vval = vval - fac * over_h<real>(phi[id] - phi[id - sy], K.hy, K.ihy, K.pow2);
-            A.v[id] = vval;
-        }
-        if (inw) {
-            wval = wval - fac * over_h<real>(phi[id] - phi[id - 1], K.hz, K.ihz, K.pow2);
-            A.w[id] = wval;
-        }
-        if (inu) {
-            uval = uval - fac * over_h<real>(phi[id] - phi[id - sx], K.hx, K.ihx, K.pow2);
-            A.u[id] = uval;
-        }
-        if (i == Ru.ie + 1 && j >= Ru.js && k >= Ru.ks) {
-            A.u[id] = uval + (real)A.scal[S_DEFICIT];
-        }
-        if (A.do_ghosts && ghost_i) {
-            if (k == Rg.ks) { A.u[id - 1] = uval; A.v[id - 1] = vval; }
-            if (k == Rg.ke) { A.u[id + 1] = uval; A.v[id + 1] = vval; }
-            if (j == Rg.js) { A.u[id - sy] = -uval; A.w[id - sy] = -wval; }
-            if (j == Rg.je) { A.u[id + sy] = -uval; A.w[id + sy] = -wval; }
-            if (i == Rg.is) { A.v[id - sx] = -vval; A.w[id - sx] = -wval; }
-        }
-    } else if (A.do_ghosts && ghost_i) {
-        const real uval = A.u[id], vval = A.v[id], wval = A.w[id];
-        if (k == Rg.ks) { A.u[id - 1] = uval; A.v[id - 1] = vval; }
-        if (k == Rg.ke) { A.u[id + 1] = uval; A.v[id + 1] = vval; }
-        if (j == Rg.js) { A.u[id - sy] = -uval; A.w[id - sy] = -wval; }
-        if (j == Rg.je) { A.u[id + sy] = -uval; A.w[id + sy] = -wval; }
-        if (i == Rg.is) { A.v[id - sx] = -vval; A.w[id - sx] = -wval; }
-    }
 
-    if (A.do_pg) {
-        const real fac = (real)(0.5 * dt * A.alpha);
-        real a, b, c;
-        if (inv) {
-            auto gp = [&](long p) { return over_h<real>(phi[p] - phi[p - sy], K.hy, K.ihy, K.pow2); };
-            const real g0 = gp(id);
-            acoef<VV, 0, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
-            real pxx = a * gp(id - sx) + b * g0 + c * gp(id + sx);
-            acoef<VV, 1, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
-            real pyy = a * gp(id - sy) + b * g0 + c * gp(id + sy);
-            acoef<VV, 2, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
-            real pzz = a * gp(id - 1) + b * g0 + c * gp(id + 1);
-            A.pgv[id] = A.pgv[id] + g0 - fac * (pyy + pxx + pzz);
-        }
-        if (inu) {
-            auto gp = [&](long p) { return over_h<real>(phi[p] - phi[p - sx], K.hx, K.ihx, K.pow2); };
-            const real g0 = gp(id);
-            acoef<VU, 0, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
-            real pxx = a * gp(id - sx) + b * g0 + c * gp(id + sx);
-            acoef<VU, 1, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
-            real pyy = a * gp(id - sy) + b * g0 + c * gp(id + sy);
-            acoef<VU, 2, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
-            real pzz = a * gp(id - 1) + b * g0 + c * gp(id + 1);
-            A.pgu[id] = A.pgu[id] + g0 - fac * (pyy + pxx + pzz);
-        }
-        if (inw) {
-            auto gp = [&](long p) { return over_h<real>(phi[p] - phi[p - 1], K.hz, K.ihz, K.pow2); };
-            const real g0 = gp(id);
-            acoef<VW, 0, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
-            real pxx = a * gp(id - sx) + b * g0 + c * gp(id + sx);
-            acoef<VW, 1, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
-            real pyy = a * gp(id - sy) + b * g0 + c * gp(id + sy);
-            acoef<VW, 2, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
-            real pzz = a * gp(id - 1) + b * g0 + c * gp(id + 1);
-            A.pgw[id] = A.pgw[id] + g0 - fac * (pyy + pxx + pzz);
+        if (do_pg) {
+            if (inv) pgv[id] = pg_update<VV, real>(K, G, phi, mc, mxy, mxz, myz, id, sx, sy, pfac, pgv[id]);
+            if (inu) pgu[id] = pg_update<VU, real>(K, G, phi, mc, mxy, mxz, myz, id, sx, sy, pfac, pgu[id]);
+            if (inw) pgw[id] = pg_update<VW, real>(K, G, phi, mc, mxy, mxz, myz, id, sx, sy, pfac, pgw[id]);
         }
     }
 }

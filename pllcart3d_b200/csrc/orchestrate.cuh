@@ -110,7 +110,8 @@ template <typename real>
 void launch_viscosity(pllgpu_ctx* ctx, const real* cn, MuPtrs<real> m, int law = -1)
 {
     dim3 blk(32, 4);
-    k_viscosity<real><<<box_grid(ctx->G.NZ, ctx->G.NY, ni(ctx->Rg) + 2, blk), blk, 0, ctx->st>>>(
+    k_viscosity<real><<<box_grid(ctx->G.NZ, ctx->G.NY, (ni(ctx->Rg) + 2 + VISC_NI - 1) / VISC_NI, blk), blk, 0,
+                        ctx->st>>>(
         ctx->G, ctx->Rg, ctx->K, law < 0 ? ctx->P.nmvp : law, cn, (real*)m.cell, (real*)m.xy, (real*)m.xz,
         (real*)m.yz, ctx->scal);
     mark(ctx, "viscosity");
@@ -143,6 +144,10 @@ void launch_umma(pllgpu_ctx* ctx, int pass, long rows, int K, const UmmaEpi& e, 
 {
     const UmmaPlan& U = ctx->um;
     const int ntiles = (int)(rows / UM_BM);
+    if (e.rows_per_plane % UM_BM) {   // the epilogue assumes whole tiles per plane
+        fail(ctx, PLLGPU_EINVAL);
+        return;
+    }
     if (ctx->P.dct_kernel == 2) {   // one tile per CTA
         const dim3 grid((unsigned)ntiles);
         if (K == 256)
@@ -237,23 +242,13 @@ template <typename real>
 void launch_project(pllgpu_ctx* ctx, double alpha, int correct, int ghosts, int pgu)
 {
     Bufs<real>& B = bufs<real>(ctx);
-    ProjectArgs<real> A;
-    A.u = q_new<real>(ctx, VU);
-    A.v = q_new<real>(ctx, VV);
-    A.w = q_new<real>(ctx, VW);
-    A.pgu = B.pg[VU];
-    A.pgv = B.pg[VV];
-    A.pgw = B.pg[VW];
-    A.phi = B.phi;
-    A.mu = mu_new<real>(ctx);
-    A.scal = ctx->scal;
-    A.alpha = alpha;
-    A.do_correct = correct;
-    A.do_ghosts = ghosts;
-    A.do_pg = pgu;
+    const MuPtrs<real> mu = mu_new<real>(ctx);
     dim3 blk(32, 4);
-    k_project<real><<<box_grid(nk(ctx->Rg), nj(ctx->Rg), ni(ctx->Rg) + 1, blk), blk, 0, ctx->st>>>(
-        ctx->G, ctx->Rg, ctx->Rv[VU], ctx->Rv[VV], ctx->Rv[VW], ctx->K, A);
+    k_project<real><<<box_grid(nk(ctx->Rg), nj(ctx->Rg), (ni(ctx->Rg) + 1 + PROJECT_NI - 1) / PROJECT_NI, blk),
+                      blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->Rv[VU], ctx->Rv[VV], ctx->Rv[VW], ctx->K,
+                                         q_new<real>(ctx, VU), q_new<real>(ctx, VV), q_new<real>(ctx, VW),
+                                         B.pg[VU], B.pg[VV], B.pg[VW], B.phi, mu.cell, mu.xy, mu.xz, mu.yz,
+                                         ctx->scal, alpha, correct, ghosts, pgu);
     mark(ctx, "project");
 }
 

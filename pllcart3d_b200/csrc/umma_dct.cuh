@@ -172,6 +172,16 @@ __device__ __forceinline__ void um_ld16(uint32_t taddr, uint32_t* r)
         : "r"(taddr));
 }
 
+// Row-major epilogue: element offset of (row 32 q, column lane) of the tile
+// starting at output row m0.  A plane holds 128 or 256 rows (a multiple of
+// the 128-row tile), so all rows of a tile lie in one plane and their offsets
+// are this origin plus rr * oq + column * on.
+__device__ __forceinline__ long tile_origin(const UmmaEpi& e, long m0, int q, int lane)
+{
+    const long plane = m0 / e.rows_per_plane, prow = m0 % e.rows_per_plane + 32 * q;
+    return plane * e.ob + prow * e.oq + (long)lane * e.on;
+}
+
 __device__ __forceinline__ float um_rna_tf32(float x)
 {
     uint32_t r;
@@ -312,6 +322,7 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
                 // memory (the pipeline stages are idle now) so that a warp
                 // stores 32 consecutive columns of one row at a time
                 float* buf = (float*)sm + (warp - 2) * 32 * 33;
+                float* o = out + tile_origin(e, m0, q, lane);
                 for (int c0 = 0; c0 < BN; c0 += 32) {
                     uint32_t v[32];
                     um_ld16(trow + c0, v);
@@ -320,13 +331,12 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
 #pragma unroll
                     for (int j = 0; j < 32; ++j) buf[lane * 33 + j] = __uint_as_float(v[j]);
                     __syncwarp();
+#pragma unroll 8
                     for (int rr = 0; rr < 32; ++rr) {
-                        const long r = m0 + 32 * q + rr;
                         float x = buf[rr * 33 + lane];
                         if (e.scale_mode == 1) x = x * e.scale;
                         else if (e.scale_mode == 2) x = x / e.scale;
-                        out[(r / e.rows_per_plane) * e.ob + (r % e.rows_per_plane) * e.oq + (long)(c0 + lane) * e.on] =
-                            x;
+                        o[(long)rr * e.oq + (long)c0 * e.on] = x;
                     }
                     __syncwarp();
                 }
@@ -518,6 +528,7 @@ __global__ void __launch_bounds__(UMP_THREADS, 1)
                     }
                 }
             } else {
+                float* o = out + tile_origin(e, m0, q, lane);
                 for (int c0 = 0; c0 < BN; c0 += 32) {
                     uint32_t v[32];
                     um_ld16(trow + c0, v);
@@ -526,13 +537,12 @@ __global__ void __launch_bounds__(UMP_THREADS, 1)
 #pragma unroll
                     for (int j = 0; j < 32; ++j) buf[lane * 33 + j] = __uint_as_float(v[j]);
                     __syncwarp();
+#pragma unroll 8
                     for (int rr = 0; rr < 32; ++rr) {
-                        const long r = m0 + 32 * q + rr;
                         float x = buf[rr * 33 + lane];
                         if (e.scale_mode == 1) x = x * e.scale;
                         else if (e.scale_mode == 2) x = x / e.scale;
-                        out[(r / e.rows_per_plane) * e.ob + (r % e.rows_per_plane) * e.oq + (long)(c0 + lane) * e.on] =
-                            x;
+                        o[(long)rr * e.oq + (long)c0 * e.on] = x;
                     }
                     __syncwarp();
                 }
