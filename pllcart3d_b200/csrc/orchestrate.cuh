@@ -52,6 +52,58 @@ void launch_explicit(pllgpu_ctx* ctx, const real* un, const real* vn, const real
     mark(ctx, lab[VAR]);
 }
 
+// the precision form's segmented solve along x (AXIS 0) or y (AXIS 1): lines
+// of LS_P * RS rows or one fewer, RS in {4, 8, 16, 32}; false: not applicable
+template <int VAR, int AXIS, int RS>
+void line_seg(pllgpu_ctx* ctx, const Rng& R, const XsweepArgs<float>& X, int n)
+{
+    const dim3 grid((nk(R) + 31) / 32, AXIS == 0 ? nj(R) : ni(R)), blk(32 * LS_P);
+    constexpr size_t smem = line_seg_smem<VAR, AXIS, RS>();
+    if (n == LS_P * RS)
+        k_line_seg<VAR, AXIS, RS, true><<<grid, blk, smem, ctx->st>>>(ctx->G, R, ctx->K, X);
+    else
+        k_line_seg<VAR, AXIS, RS, false><<<grid, blk, smem, ctx->st>>>(ctx->G, R, ctx->K, X);
+}
+
+template <int VAR, int AXIS>
+bool launch_line_seg(pllgpu_ctx* ctx, const Rng& R, const XsweepArgs<float>& X)
+{
+    if (ctx->P.exact_dct || ctx->nelem >= (1L << 31)) return false;
+    const int n = AXIS == 0 ? ni(R) : nj(R);
+    const int rs = (n + LS_P - 1) / LS_P;   // rows per segment
+    if (rs != 4 && rs != 8 && rs != 16 && rs != 32) return false;
+    if (n != LS_P * rs) {
+        // one row short: the kernel loads the row past the line (and the
+        // viscosity family one beyond it), which must lie in the padded box
+        const int start = AXIS == 0 ? R.is : R.js, top = AXIS == 0 ? ctx->G.NX - 1 : ctx->G.NY - 1;
+        if (n != LS_P * rs - 1 || start + LS_P * rs + LineCoef<VAR, AXIS>::off > top) return false;
+    }
+    if (rs == 4) line_seg<VAR, AXIS, 4>(ctx, R, X, n);
+    else if (rs == 8) line_seg<VAR, AXIS, 8>(ctx, R, X, n);
+    else if (rs == 16) line_seg<VAR, AXIS, 16>(ctx, R, X, n);
+    else line_seg<VAR, AXIS, 32>(ctx, R, X, n);
+    return true;
+}
+
+// shared-memory limits of the segmented solves (tiles pass 48 KB for RS 16
+// and 32)
+template <int VAR, int AXIS, int RS>
+void line_seg_attr()
+{
+    const int b = (int)line_seg_smem<VAR, AXIS, RS>();
+    cudaFuncSetAttribute(k_line_seg<VAR, AXIS, RS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    cudaFuncSetAttribute(k_line_seg<VAR, AXIS, RS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+}
+
+template <int VAR>
+void line_seg_attrs()
+{
+    line_seg_attr<VAR, 0, 16>();
+    line_seg_attr<VAR, 0, 32>();
+    line_seg_attr<VAR, 1, 16>();
+    line_seg_attr<VAR, 1, 32>();
+}
+
 template <typename real, int VAR>
 void launch_implicit(pllgpu_ctx* ctx, double g, double r)
 {
@@ -76,9 +128,10 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
     const int lb = tune_line_block(ctx->tune_line);
     bool ydone = false;
     if constexpr (std::is_same<real, float>::value) {
-        // the precision form's partitioned warp solve; for momentum the
-        // prefetching Thomas sweep measures faster and stays
-        if (VAR == VC && nj(R) <= ZP_MAX && nj(R) >= 2 * (ZP_MAX / 32) && !ctx->P.exact_dct) {
+        // the precision form's partitioned solves: segmented when the line
+        // length allows, else for concentration the warp solve of short lines
+        ydone = launch_line_seg<VAR, 1>(ctx, R, X);
+        if (!ydone && VAR == VC && nj(R) <= ZP_MAX && nj(R) >= 2 * (ZP_MAX / 32) && !ctx->P.exact_dct) {
             k_adi_y_part<VAR><<<dim3((nk(R) + 31) / 32, ni(R)), 256, adi_y_part_smem(), ctx->st>>>(
                 ctx->G, R, ctx->K, X.mu, B.S, ctx->scal, alpha);
             ydone = true;
@@ -102,7 +155,10 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
             ctx->G, R, ctx->K, X.mu, B.S, B.cc, ctx->scal, alpha);
     }
     mark(ctx, lz[VAR]);
-    k_line_pf<VAR, 0, real><<<dim3((nk(R) + lb - 1) / lb, nj(R)), lb, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
+    bool xdone = false;
+    if constexpr (std::is_same<real, float>::value) xdone = launch_line_seg<VAR, 0>(ctx, R, X);
+    if (!xdone)
+        k_line_pf<VAR, 0, real><<<dim3((nk(R) + lb - 1) / lb, nj(R)), lb, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
     mark(ctx, lx[VAR]);
 }
 
@@ -687,6 +743,10 @@ bool alloc_state(pllgpu_ctx* c)
         cudaFuncSetAttribute(k_adi_y_part<VU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adi_y_part_smem());
         cudaFuncSetAttribute(k_adi_y_part<VV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adi_y_part_smem());
         cudaFuncSetAttribute(k_adi_y_part<VW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adi_y_part_smem());
+        line_seg_attrs<VC>();
+        line_seg_attrs<VU>();
+        line_seg_attrs<VV>();
+        line_seg_attrs<VW>();
     }
     cudaFuncSetAttribute(k_adi_z_tiled<VC, real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)adi_z_smem_bytes<VC, real>());

@@ -1252,5 +1252,300 @@ __global__ void __launch_bounds__(128) k_line_pf(Geo G, Rng R, Consts K, XsweepA
 
 }
 
+// ---------------------------------------------------------------------------
+// The precision form's line solve along a strided axis (x or y) by a
+// partition method: a block owns 32 neighbouring lines (lane = line, adjacent
+// k, so every row access is one coalesced 128-byte transaction) and cuts each
+// line into LS_P segments of RS rows, one warp per segment.  A thread keeps
+// its segment's right-hand side in registers; its viscosity rows (momentum)
+// and, for the x sweep, its q_old rows are copied into shared memory by
+// cp.async, each thread copying and later reading only its own rows.  The
+// thread eliminates the interior rows in terms of the segment's first row
+// (its separator) and the next segment's, the LS_P separator equations of
+// every line are solved by one thread per line through shared memory, and
+// each thread finishes its rows with the separators known.  Every input is
+// read once from HBM and every output written once (the sequential sweep
+// also writes and re-reads c' and the eliminated rhs).  Same coefficients
+// and closures as k_line_pf (x: convective outflow, q_new = q_old + delta,
+// concentration's Neumann ghosts; y: in place into S); FP32-level agreement
+// with the sequential sweep, not bitwise.
+// ---------------------------------------------------------------------------
+constexpr int LS_P = 16;   // segments per line = warps per block
+
+// dynamic shared memory of k_line_seg: the viscosity family's rows (RS + 1
+// per thread, momentum) then the x sweep's q_old rows (RS per thread)
+template <int VAR, int AXIS, int RS>
+constexpr size_t line_seg_smem()
+{
+    return sizeof(float) * 32 * LS_P * ((VAR != VC ? RS + 1 : 0) + (AXIS == 0 ? RS : 0));
+}
+
+__device__ __forceinline__ void ls_cp_async4(float* dst, const float* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+
+// an optimisation barrier on x: later reads cannot reuse values computed
+// from it before (keeps each sweep recomputing its row coefficients instead
+// of holding four per row in registers; a "memory" clobber does the same
+// for the shared-memory rows)
+__device__ __forceinline__ void ls_fresh(float& x) { asm volatile("" : "+f"(x)); }
+
+// FULL: the line has LS_P * RS rows; else LS_P * RS - 1 and the last
+// segment's last row is an identity row (its loads read the row past the
+// line, which the host checks lies inside the padded box)
+template <int VAR, int AXIS, int RS, bool FULL>
+__global__ void __launch_bounds__(32 * LS_P) k_line_seg(Geo G, Rng R, Consts K, XsweepArgs<float> A)
+{
+    __shared__ float eq[4][LS_P][32];       // separator equations
+    __shared__ float tail[3][LS_P][32];     // last interior row of each segment
+    __shared__ float sep[LS_P + 1][32];     // separator values
+    extern __shared__ float ls_dyn[];       // [row][thread] tiles: viscosity, then q_old (x)
+    constexpr int LO = Closure<VAR, AXIS>::lo, HI = Closure<VAR, AXIS>::hi;
+    constexpr int OFF = LineCoef<VAR, AXIS>::off;
+    constexpr int TS = 32 * LS_P;
+    const int lane = threadIdx.x & 31, l = threadIdx.x >> 5;
+    const int k = R.ks + blockIdx.x * 32 + lane;
+    const int o = blockIdx.y;   // j (AXIS 0) or i (AXIS 1) offset
+    const bool live = k <= R.ke;
+    const bool last_seg = l == LS_P - 1;
+    constexpr int n = FULL ? LS_P * RS : LS_P * RS - 1;
+    // offsets fit in 32 bits (the host checks the field size)
+    const int st = AXIS == 0 ? (int)G.sx : (int)G.sy;
+    const long base = AXIS == 0 ? (long)R.is * G.sx + (long)(R.js + o) * G.sy + k
+                                : (long)(R.is + o) * G.sx + (long)R.js * G.sy + k;
+    const long seg = base + (long)(l * RS) * st;
+    const float dt = (float)A.scal[S_DT];
+    const float fac = (float)(0.5 * A.scal[S_DT] * A.alpha);
+    const float* __restrict__ fam = VAR == VC ? nullptr : line_family<VAR, AXIS, float>(A.mu);
+    float* __restrict__ S = A.S;
+    // this thread's row e of the tiles: mym[e * TS], myq[e * TS]
+    float* mym = ls_dyn + threadIdx.x;
+    float* myq = ls_dyn + (VAR != VC ? (RS + 1) * TS : 0) + threadIdx.x;
+
+    if (VAR != VC) {
+        if (live) {
+            const float* mp = fam + seg + OFF * st;
+#pragma unroll
+            for (int e = 0; e <= RS; ++e) ls_cp_async4(mym + e * TS, mp + e * st);
+        } else {
+#pragma unroll
+            for (int e = 0; e <= RS; ++e) mym[e * TS] = 0.f;
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    if (AXIS == 0 && live) {
+#pragma unroll
+        for (int e = 0; e < RS; ++e) ls_cp_async4(myq + e * TS, A.q + seg + e * st);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    float rS[RS];
+    {
+        const float* sp = S + seg;
+#pragma unroll
+        for (int e = 0; e < RS; ++e) rS[e] = live ? sp[e * st] : 0.f;
+    }
+
+    // convective outflow value (x): the thread that owns the line's last row
+    float boun = 0.f;
+    if (AXIS == 0 && live && last_seg) {
+        const long rb = base + (long)n * st;
+        float Hb = -(float)A.scal[S_VBULK] * (A.q[rb] - A.q[rb - st]);
+        Hb = over_h<float>(Hb, K.hx, K.ihx, K.pow2);
+        A.H[rb] = Hb;
+        boun = dt * ((float)A.g * Hb + (float)A.r * A.Hm[rb]);
+        A.qn[rb] = A.q[rb] + boun;
+    }
+    if (VAR != VC) {
+        // the viscosity rows have landed (the q rows may still be in flight)
+        if (AXIS == 0 && live) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+
+    // row e of this segment: (la, lb, lc, lr) with the line's closures; la of
+    // the line's first row and lc of its last are dropped (the sequential
+    // sweep multiplies them by zero)
+    auto row = [&](int e, float& la, float& lb, float& lc, float& lr) {
+        if (!FULL && last_seg && e == RS - 1) {
+            la = 0.f;
+            lb = 1.0f;
+            lc = 0.f;
+            lr = 0.f;
+            return;
+        }
+        float a, c;
+        line_ac<VAR, AXIS, float>(K, VAR == VC ? 0.f : mym[e * TS], VAR == VC ? 0.f : mym[(e + 1) * TS], a, c);
+        const float b = -(a + c);
+        la = -fac * a;
+        lb = 1.0f - fac * b;
+        lc = -fac * c;
+        lr = rS[e];
+        if (e == 0 && l == 0) {
+            if (LO == 1) lb += la;
+            else if (LO == 2) lb -= la;
+            la = 0.f;
+        }
+        if (last_seg && e == (FULL ? RS - 1 : RS - 2)) {
+            if (AXIS == 0) lr -= lc * boun;
+            else if (HI == 1) lb += lc;
+            else if (HI == 2) lb -= lc;
+            lc = 0.f;
+        }
+    };
+    auto fresh = [&]() {
+#pragma unroll
+        for (int e = 0; e < RS; ++e) ls_fresh(rS[e]);
+        asm volatile("" ::: "memory");
+    };
+
+    // interior rows top-down: x_e = rh - ah S_l - ch x_{e+1}; at the last
+    // interior row x_{e+1} is the next separator
+    float gL, vL, wL;
+    {
+        float la, lb, lc, lr;
+        row(1, la, lb, lc, lr);
+        float ib = __fdividef(1.0f, lb);
+        float ch = lc * ib, rh = lr * ib, ah = la * ib;
+#pragma unroll
+        for (int e = 2; e < RS; ++e) {
+            row(e, la, lb, lc, lr);
+            ib = __fdividef(1.0f, lb - la * ch);
+            rh = (lr - la * rh) * ib;
+            ah = -la * ah * ib;
+            ch = lc * ib;
+        }
+        gL = rh;
+        vL = ah;
+        wL = ch;
+    }
+    fresh();
+    // bottom-up: x_e = rb - ab S_l - cb S_{l+1} down to the first interior row
+    float g1, v1, w1;
+    {
+        float la, lb, lc, lr;
+        row(RS - 1, la, lb, lc, lr);
+        float ib = __fdividef(1.0f, lb);
+        float rb = lr * ib, cb = lc * ib, ab = la * ib;
+#pragma unroll
+        for (int e = RS - 2; e >= 1; --e) {
+            row(e, la, lb, lc, lr);
+            ib = __fdividef(1.0f, lb - lc * ab);
+            rb = (lr - lc * rb) * ib;
+            cb = -lc * cb * ib;
+            ab = la * ib;
+        }
+        g1 = rb;
+        v1 = ab;
+        w1 = cb;
+    }
+    fresh();
+    tail[0][l][lane] = gL;
+    tail[1][l][lane] = vL;
+    tail[2][l][lane] = wL;
+    __syncthreads();
+    {
+        // separator row: a0 x_{-1} + b0 S_l + c0 x_1 = r0 with x_{-1} the
+        // previous segment's last interior row
+        float a0, b0, c0, r0;
+        row(0, a0, b0, c0, r0);
+        float gp = 0.f, vp = 0.f, wp = 0.f;
+        if (l > 0) {
+            gp = tail[0][l - 1][lane];
+            vp = tail[1][l - 1][lane];
+            wp = tail[2][l - 1][lane];
+        }
+        eq[0][l][lane] = -a0 * vp;
+        eq[1][l][lane] = b0 - a0 * wp - c0 * v1;
+        eq[2][l][lane] = -c0 * w1;
+        eq[3][l][lane] = r0 - a0 * gp - c0 * g1;
+    }
+    __syncthreads();
+    if (l == 0) {
+        // the LS_P separator equations of this lane's line (Thomas)
+        float cp[LS_P], rp[LS_P];
+        float ib = __fdividef(1.0f, eq[1][0][lane]);
+        cp[0] = eq[2][0][lane] * ib;
+        rp[0] = eq[3][0][lane] * ib;
+#pragma unroll
+        for (int t = 1; t < LS_P; ++t) {
+            const float al = eq[0][t][lane];
+            ib = __fdividef(1.0f, eq[1][t][lane] - al * cp[t - 1]);
+            cp[t] = eq[2][t][lane] * ib;
+            rp[t] = (eq[3][t][lane] - al * rp[t - 1]) * ib;
+        }
+        float x = rp[LS_P - 1];
+        sep[LS_P - 1][lane] = x;
+        sep[LS_P][lane] = 0.f;
+#pragma unroll
+        for (int t = LS_P - 2; t >= 0; --t) {
+            x = rp[t] - cp[t] * x;
+            sep[t][lane] = x;
+        }
+    }
+    __syncthreads();
+    if (!live) return;
+    const float Sl = sep[l][lane], Sn = sep[l + 1][lane];
+    fresh();
+
+    // interior rows with both separators known: Thomas with x_0 = S_l and
+    // x_RS = S_{l+1}; c' in cq, the eliminated rhs replaces rS
+    float cq[RS];
+    {
+        float la, lb, lc, lr;
+        row(1, la, lb, lc, lr);
+        float ib = __fdividef(1.0f, lb);
+        cq[1] = lc * ib;
+        rS[1] = (lr - la * Sl) * ib;
+#pragma unroll
+        for (int e = 2; e < RS; ++e) {
+            row(e, la, lb, lc, lr);
+            ib = __fdividef(1.0f, lb - la * cq[e - 1]);
+            cq[e] = lc * ib;
+            rS[e] = (lr - la * rS[e - 1]) * ib;
+        }
+    }
+    if (AXIS == 0) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    // q_new (x; for c also its Neumann ghosts in y then z, as k_line_pf) or
+    // the solution in place (y)
+    const int jl = R.js + o;
+    const bool jlo = AXIS == 0 && VAR == VC && jl == R.js, jhi = AXIS == 0 && VAR == VC && jl == R.je;
+    const bool klo = AXIS == 0 && VAR == VC && k == R.ks, khi = AXIS == 0 && VAR == VC && k == R.ke;
+    const bool edge = jlo | jhi | klo | khi;
+    auto put = [&](int e, float x) {
+        if (!FULL && last_seg && e == RS - 1) return;
+        const long id = seg + e * st;
+        if (AXIS != 0) {
+            S[id] = x;
+            return;
+        }
+        const float v = myq[e * TS] + x;
+        A.qn[id] = v;
+        if (edge) {
+            const long sy = G.sy;
+            if (jlo) A.qn[id - sy] = v;
+            if (jhi) A.qn[id + sy] = v;
+            if (klo) {
+                A.qn[id - 1] = v;
+                if (jlo) A.qn[id - sy - 1] = v;
+                if (jhi) A.qn[id + sy - 1] = v;
+            }
+            if (khi) {
+                A.qn[id + 1] = v;
+                if (jlo) A.qn[id - sy + 1] = v;
+                if (jhi) A.qn[id + sy + 1] = v;
+            }
+        }
+    };
+    float x = Sn;
+#pragma unroll
+    for (int e = RS - 1; e >= 1; --e) {
+        x = rS[e] - cq[e] * x;
+        put(e, x);
+    }
+    put(0, Sl);
+}
+
 }  // namespace
 }  // namespace pll
