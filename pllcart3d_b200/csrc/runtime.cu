@@ -186,6 +186,11 @@ pllgpu_ctx* pllgpu_create(const pllgpu_params* p, int device)
     G.dy = (p->Y2 - p->Y1) / (double)p->ny;
     G.dz = (p->Z2 - p->Z1) / (double)p->nz;
     ctx->nelem = (long)G.NX * G.sx;
+    if (ctx->nelem >= (1L << 31)) {   // kernels index a field with 32-bit offsets
+        cudaStreamDestroy(ctx->st);
+        delete ctx;
+        return nullptr;
+    }
     // index ranges, simulation_setup pllcart3d.c:405-431 (one rank)
     Rng& Rg = ctx->Rg;
     Rg.is = 3; Rg.ie = p->nx + 2; Rg.js = 1; Rg.je = p->ny; Rg.ks = 1; Rg.ke = p->nz;

@@ -108,3 +108,28 @@ def test_persistent_tcgen05_dct_equals_per_tile(name):
         assert s.status() == 0
     for f in ("phi", "u_new", "v_new", "w_new", "c_new"):
         assert np.array_equal(a.get(f), b.get(f)), f
+
+
+@pytest.mark.parametrize("name", ["fingering-64x64x64", "fingering-512x16x16", "fingering-16x512x16"])
+def test_segmented_line_solves_one_step(name):
+    """The precision form's segmented x / y line solves (lines of 64 and
+    512 rows, and the one-row-shorter staggered components) against the FP64
+    step, next to the precision form's sequential path (exact_dct: Thomas
+    sweeps and sequential-order DCT sums): both carry FP32-level errors of
+    the same size (large relative to a component that is nearly zero on a
+    grid one cell wide in z)."""
+    from pllcart3d_b200.solver import Solver
+
+    wl = workload(name)
+    ic = workload_fields(wl)
+    ref = Solver(wl.params, precision="fp64")
+    seg = Solver(wl.params, precision="mixed")
+    seq = Solver(wl.params, precision="mixed", exact_dct=True)
+    for s in (ref, seg, seq):
+        s.load_ic(ic)
+        s.step(1)
+        assert s.status() == 0
+    for f in ("c_new", "u_new", "v_new", "w_new"):
+        e_seg = rel_maxnorm(seg.get(f), ref.get(f))
+        e_seq = rel_maxnorm(seq.get(f), ref.get(f))
+        assert e_seg <= 3.0 * e_seq + 1e-6, (f, e_seg, e_seq)
