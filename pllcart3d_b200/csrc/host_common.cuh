@@ -46,7 +46,9 @@ template <typename T>
 T* dalloc(pllgpu_ctx* ctx, long n)
 {
     void* p = nullptr;
-    const size_t bytes = sizeof(T) * (size_t)(n > 0 ? n : 1);
+    // 1 KB of zeroed slack past the end: kernels that compute cell pairs
+    // (k_explicit2) read, and never write, up to 66 elements beyond a field
+    const size_t bytes = sizeof(T) * (size_t)(n > 0 ? n : 1) + 1024;
     if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
     cudaMemset(p, 0, bytes);
     ctx->allocs.push_back(p);

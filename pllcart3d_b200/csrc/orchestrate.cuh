@@ -47,8 +47,16 @@ void launch_explicit(pllgpu_ctx* ctx, const real* un, const real* vn, const real
     A.alpha = g + r;
     int bx, by;
     tune_exp_block(ctx->tune_exp, bx, by);
-    const dim3 blk(bx, by);
-    k_explicit<VAR, real><<<box_grid(nk(R), nj(R), ni(R), blk), blk, 0, ctx->st>>>(ctx->G, R, ctx->K, A);
+    if constexpr (std::is_same<real, float>::value) {
+        // cell pairs (k, k + EP_DK): blocks of EP_DK x rows, the same threads
+        // per block as the tuned shape
+        const dim3 blk(EP_DK, bx * by / EP_DK);
+        const dim3 grid((nk(R) + 2 * EP_DK - 1) / (2 * EP_DK), (nj(R) + blk.y - 1) / blk.y, ni(R));
+        k_explicit2<VAR><<<grid, blk, 0, ctx->st>>>(ctx->G, R, ctx->K, A);
+    } else {
+        const dim3 blk(bx, by);
+        k_explicit<VAR, real><<<box_grid(nk(R), nj(R), ni(R), blk), blk, 0, ctx->st>>>(ctx->G, R, ctx->K, A);
+    }
     mark(ctx, lab[VAR]);
 }
 

@@ -383,6 +383,247 @@ __global__ void __launch_bounds__(128) k_explicit(Geo G, Rng R, Consts K,
     A.S[id] = S;
 }
 
+// ---------------------------------------------------------------------------
+// The precision form's explicit operator on cell pairs with packed FP32x2
+// arithmetic.  k_explicit in FP32 is issue-bound (~620 instructions per
+// cell, 40 % of them FP32 add / multiply / fma), so each thread takes two
+// cells, (i, j, k) and (i, j, k + 32), and runs the shared arithmetic once on
+// both through sm_100's paired instructions (__fadd2_rn / __fmul2_rn /
+// __ffma2_rn, one instruction for two FP32 operations); the second cell's
+// loads are the first cell's addresses plus 128 bytes, so its address
+// arithmetic is free too.  Every formula, constant and closure is
+// k_explicit's; the two differ only in where a multiply and an add are fused
+// (FP32 rounding level).  Points past the line's end: the second cell of the
+// last tile may lie past ke; it is computed from reads into the row beyond
+// (every device array carries zeroed slack past its end for this) and never
+// stored.
+// ---------------------------------------------------------------------------
+struct f2 {
+    float2 v;
+};
+__device__ __forceinline__ f2 F2(float a, float b) { return f2{make_float2(a, b)}; }
+__device__ __forceinline__ f2 S2(float a) { return f2{make_float2(a, a)}; }
+__device__ __forceinline__ f2 operator+(f2 a, f2 b) { return f2{__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ f2 operator*(f2 a, f2 b) { return f2{__fmul2_rn(a.v, b.v)}; }
+// a - b, and a + b * c, with one rounding each
+__device__ __forceinline__ f2 operator-(f2 a, f2 b) { return f2{__ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v)}; }
+__device__ __forceinline__ f2 fma2(f2 b, f2 c, f2 a) { return f2{__ffma2_rn(b.v, c.v, a.v)}; }
+__device__ __forceinline__ f2 neg2(f2 a) { return a * S2(-1.f); }
+
+constexpr int EP_DK = 32;   // k distance of a thread's two cells
+
+__device__ __forceinline__ f2 ld2(const float* __restrict__ p, long id) { return F2(p[id], p[id + EP_DK]); }
+
+// packed weno5<float>: the same weights with the approximate divisions per
+// component
+__device__ __forceinline__ f2 weno5_2(f2 v0, f2 v1, f2 v2, f2 v3, f2 v4)
+{
+    const f2 con1 = S2((float)(1.0 / 6.0)), con2 = S2((float)(13.0 / 12.0)), con3 = S2(0.25f);
+    const f2 q0 = v0 * v0, q1 = v1 * v1, q2 = v2 * v2, q3 = v3 * v3, q4 = v4 * v4;
+    const f2 maxd = F2(fmaxf(fmaxf(fmaxf(q0.v.x, q1.v.x), fmaxf(q2.v.x, q3.v.x)), q4.v.x),
+                       fmaxf(fmaxf(fmaxf(q0.v.y, q1.v.y), fmaxf(q2.v.y, q3.v.y)), q4.v.y));
+    const f2 c1 = con1 * fma2(S2(2.0f), v0, fma2(S2(-7.0f), v1, S2(11.0f) * v2));
+    const f2 c2 = con1 * fma2(S2(2.0f), v3, fma2(S2(5.0f), v2, neg2(v1)));
+    const f2 c3 = con1 * fma2(S2(2.0f), v2, fma2(S2(5.0f), v3, neg2(v4)));
+    f2 t1 = fma2(S2(-2.0f), v1, v0) + v2, t2 = fma2(S2(3.0f), v2, fma2(S2(-4.0f), v1, v0));
+    const f2 s1 = fma2(con2 * t1, t1, con3 * t2 * t2);
+    t1 = fma2(S2(-2.0f), v2, v1) + v3;
+    t2 = v1 - v3;
+    const f2 s2 = fma2(con2 * t1, t1, con3 * t2 * t2);
+    t1 = fma2(S2(-2.0f), v3, v2) + v4;
+    t2 = fma2(S2(-4.0f), v3, S2(3.0f) * v2) + v4;
+    const f2 s3 = fma2(con2 * t1, t1, con3 * t2 * t2);
+    const f2 eps = fma2(S2(1.0e-6f), maxd, S2(1.0e-18f));
+    const f2 e1 = s1 + eps, e2 = s2 + eps, e3 = s3 + eps;
+    const f2 d1 = e1 * e1, d2 = e2 * e2, d3 = e3 * e3;
+    const f2 a1 = S2(0.1f) * F2(__fdividef(1.0f, d1.v.x), __fdividef(1.0f, d1.v.y));
+    const f2 a2 = S2(0.6f) * F2(__fdividef(1.0f, d2.v.x), __fdividef(1.0f, d2.v.y));
+    const f2 a3 = S2(0.3f) * F2(__fdividef(1.0f, d3.v.x), __fdividef(1.0f, d3.v.y));
+    const f2 num = fma2(a3, c3, fma2(a2, c2, a1 * c1));
+    const f2 den = a1 + a2 + a3;
+    return num * F2(__fdividef(1.0f, den.v.x), __fdividef(1.0f, den.v.y));
+}
+
+template <int VAR, int AXIS>
+__device__ __forceinline__ f2 adv_vel2(const float* __restrict__ self, const float* __restrict__ un,
+                                       const float* __restrict__ vn, const float* __restrict__ wn, long id, long sx,
+                                       long sy)
+{
+    const f2 h = S2(0.5f), q = S2(0.25f);
+    if (VAR == VC) {
+        if (AXIS == 0) return h * (ld2(un, id + sx) + ld2(un, id));
+        if (AXIS == 1) return h * (ld2(vn, id + sy) + ld2(vn, id));
+        return h * (ld2(wn, id + 1) + ld2(wn, id));
+    } else if (VAR == VU) {
+        if (AXIS == 0) return ld2(self, id);
+        if (AXIS == 1) return q * (ld2(vn, id - sx) + ld2(vn, id) + ld2(vn, id + sy) + ld2(vn, id - sx + sy));
+        return q * (ld2(wn, id - sx) + ld2(wn, id) + ld2(wn, id + 1) + ld2(wn, id - sx + 1));
+    } else if (VAR == VV) {
+        if (AXIS == 0) return q * (ld2(un, id - sy) + ld2(un, id + sx - sy) + ld2(un, id) + ld2(un, id + sx));
+        if (AXIS == 1) return ld2(self, id);
+        return q * (ld2(wn, id - sy) + ld2(wn, id - sy + 1) + ld2(wn, id) + ld2(wn, id + 1));
+    } else {
+        if (AXIS == 0) return q * (ld2(un, id - 1) + ld2(un, id + sx - 1) + ld2(un, id) + ld2(un, id + sx));
+        if (AXIS == 1) return q * (ld2(vn, id - 1) + ld2(vn, id) + ld2(vn, id + sy - 1) + ld2(vn, id + sy));
+        return ld2(self, id);
+    }
+}
+
+// upwind derivative of both cells along AXIS; m is the first cell's line
+// position (the second's is m + EP_DK along z, m along x and y).  Pairs with
+// a cell in the ENO-2 band take upwind_deriv per cell.
+template <int AXIS>
+__device__ __forceinline__ f2 upwind_deriv2(const float* __restrict__ q, const Geo& G, const Rng& R,
+                                            const Consts& K, long id, int m, f2 vv)
+{
+    const int s = AXIS == 0 ? R.is : AXIS == 1 ? R.js : R.ks;
+    const int e = AXIS == 0 ? R.ie : AXIS == 1 ? R.je : R.ke;
+    const int mb = AXIS == 2 ? m + EP_DK : m;
+    const bool eno = (m <= s + 1) | (m >= e - 1) | (mb <= s + 1) | (mb >= e - 1);
+    if (eno)
+        return F2(upwind_deriv<AXIS, float>(q, G, R, K, id, m, vv.v.x),
+                  upwind_deriv<AXIS, float>(q, G, R, K, id + EP_DK, mb, vv.v.y));
+    const long st = AXIS == 0 ? G.sx : AXIS == 1 ? G.sy : 1;
+    const f2 ih = S2((float)(AXIS == 0 ? K.ihx : AXIS == 1 ? K.ihy : K.ihz));
+    f2 d[6];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+        const long p = id + (long)(t - 3) * st;
+        d[t] = (ld2(q, p + st) - ld2(q, p)) * ih;
+    }
+    const bool ua = vv.v.x >= 0.f, ub = vv.v.y >= 0.f;
+    auto pick = [&](int up, int dn) { return F2(ua ? d[up].v.x : d[dn].v.x, ub ? d[up].v.y : d[dn].v.y); };
+    return weno5_2(pick(0, 5), pick(1, 4), pick(2, 3), pick(3, 2), pick(4, 1));
+}
+
+template <int VAR, int AXIS>
+__device__ __forceinline__ void acoef2(const Consts& K, const Geo& G, const MuPtrs<float>& mu, long id, f2& a,
+                                       f2& b, f2& c)
+{
+    const long sx = G.sx, sy = G.sy;
+    const f2 ihx = S2((float)K.ihx), ihy = S2((float)K.ihy), ihz = S2((float)K.ihz);
+    if (VAR == VC) {
+        a = c = S2((float)(AXIS == 0 ? K.cdx : AXIS == 1 ? K.cdy : K.cdz));
+    } else if (VAR == VU) {
+        if (AXIS == 0) {
+            a = S2((float)K.d2x) * ld2(mu.cell, id - sx) * ihx;
+            c = S2((float)K.d2x) * ld2(mu.cell, id) * ihx;
+        } else if (AXIS == 1) {
+            a = S2((float)K.d1y) * ld2(mu.xy, id) * ihy;
+            c = S2((float)K.d1y) * ld2(mu.xy, id + sy) * ihy;
+        } else {
+            a = S2((float)K.d1z) * ld2(mu.xz, id) * ihz;
+            c = S2((float)K.d1z) * ld2(mu.xz, id + 1) * ihz;
+        }
+    } else if (VAR == VV) {
+        if (AXIS == 0) {
+            a = S2((float)K.d1x) * ld2(mu.xy, id) * ihx;
+            c = S2((float)K.d1x) * ld2(mu.xy, id + sx) * ihx;
+        } else if (AXIS == 1) {
+            a = S2((float)K.d2y) * ld2(mu.cell, id - sy) * ihy;
+            c = S2((float)K.d2y) * ld2(mu.cell, id) * ihy;
+        } else {
+            a = S2((float)K.d1z) * ld2(mu.yz, id) * ihz;
+            c = S2((float)K.d1z) * ld2(mu.yz, id + 1) * ihz;
+        }
+    } else {
+        if (AXIS == 0) {
+            a = S2((float)K.d1x) * ld2(mu.xz, id) * ihx;
+            c = S2((float)K.d1x) * ld2(mu.xz, id + sx) * ihx;
+        } else if (AXIS == 1) {
+            a = S2((float)K.d1y) * ld2(mu.yz, id) * ihy;
+            c = S2((float)K.d1y) * ld2(mu.yz, id + sy) * ihy;
+        } else {
+            a = S2((float)K.d2z) * ld2(mu.cell, id - 1) * ihz;
+            c = S2((float)K.d2z) * ld2(mu.cell, id) * ihz;
+        }
+    }
+    b = neg2(a + c);
+}
+
+// grid: x over k in tiles of 2 * EP_DK (blockDim.x == EP_DK), y over j, z over i
+template <int VAR>
+__global__ void __launch_bounds__(128) k_explicit2(Geo G, Rng R, Consts K, ExplicitArgs<float> A)
+{
+    const int k = R.ks + blockIdx.x * (2 * EP_DK) + threadIdx.x;
+    const int j = R.js + blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = R.is + blockIdx.z;
+    if (k > R.ke || j > R.je) return;
+    const bool live_b = k + EP_DK <= R.ke;
+    const long sx = G.sx, sy = G.sy;
+    const long id = (long)i * sx + (long)j * sy + k;
+    const float* __restrict__ q = A.q;
+
+    const f2 vx = adv_vel2<VAR, 0>(q, A.un, A.vn, A.wn, id, sx, sy);
+    const f2 cx = vx * upwind_deriv2<0>(q, G, R, K, id, i, vx);
+    const f2 vy = adv_vel2<VAR, 1>(q, A.un, A.vn, A.wn, id, sx, sy);
+    const f2 cy = vy * upwind_deriv2<1>(q, G, R, K, id, j, vy);
+    const f2 vz = adv_vel2<VAR, 2>(q, A.un, A.vn, A.wn, id, sx, sy);
+    const f2 cz = vz * upwind_deriv2<2>(q, G, R, K, id, k, vz);
+    const f2 ct = cz + cx + cy;
+    f2 H;
+    if (VAR == VC) {
+        H = neg2(ct);
+    } else {
+        const float* __restrict__ un = A.un;
+        const float* __restrict__ vn = A.vn;
+        const float* __restrict__ wn = A.wn;
+        f2 s1, s2, s3, s4;
+        if (VAR == VU) {
+            s1 = S2((float)K.xuv) * ld2(A.mu.xy, id + sy) * (ld2(vn, id + sy) - ld2(vn, id - sx + sy));
+            s2 = S2((float)K.xuv) * ld2(A.mu.xy, id) * (ld2(vn, id) - ld2(vn, id - sx));
+            s3 = S2((float)K.xuw) * ld2(A.mu.xz, id + 1) * (ld2(wn, id + 1) - ld2(wn, id - sx + 1));
+            s4 = S2((float)K.xuw) * ld2(A.mu.xz, id) * (ld2(wn, id) - ld2(wn, id - sx));
+        } else if (VAR == VV) {
+            s1 = S2((float)K.xvu) * ld2(A.mu.xy, id + sx) * (ld2(un, id + sx) - ld2(un, id + sx - sy));
+            s2 = S2((float)K.xvu) * ld2(A.mu.xy, id) * (ld2(un, id) - ld2(un, id - sy));
+            s3 = S2((float)K.xvw) * ld2(A.mu.yz, id + 1) * (ld2(wn, id + 1) - ld2(wn, id - sy + 1));
+            s4 = S2((float)K.xvw) * ld2(A.mu.yz, id) * (ld2(wn, id) - ld2(wn, id - sy));
+        } else {
+            s1 = S2((float)K.xwu) * ld2(A.mu.xz, id + sx) * (ld2(un, id + sx) - ld2(un, id + sx - 1));
+            s2 = S2((float)K.xwu) * ld2(A.mu.xz, id) * (ld2(un, id) - ld2(un, id - 1));
+            s3 = S2((float)K.xwv) * ld2(A.mu.yz, id + sy) * (ld2(vn, id + sy) - ld2(vn, id + sy - 1));
+            s4 = S2((float)K.xwv) * ld2(A.mu.yz, id) * (ld2(vn, id) - ld2(vn, id - 1));
+        }
+        H = neg2(ct) + s1 - s2 + s3 - s4;
+    }
+    A.H[id] = H.v.x;
+    if (live_b) A.H[id + EP_DK] = H.v.y;
+
+    // right-hand side dt*(gamma H + rho H_old + alpha A q_old + alpha body)
+    const f2 dt = S2((float)A.scal[S_DT]);
+    const f2 alpha = S2((float)A.alpha);
+    const f2 conv = fma2(S2((float)A.r), ld2(A.Hm, id), S2((float)A.g) * H);
+    const f2 q0 = ld2(q, id);
+    f2 a, b, c;
+    acoef2<VAR, 0>(K, G, A.mu, id, a, b, c);
+    const f2 ax = fma2(c, ld2(q, id + sx), fma2(b, q0, a * ld2(q, id - sx)));
+    acoef2<VAR, 1>(K, G, A.mu, id, a, b, c);
+    const f2 ay = fma2(c, ld2(q, id + sy), fma2(b, q0, a * ld2(q, id - sy)));
+    acoef2<VAR, 2>(K, G, A.mu, id, a, b, c);
+    const f2 az = fma2(c, ld2(q, id + 1), fma2(b, q0, a * ld2(q, id - 1)));
+    const f2 diff = alpha * (ax + ay + az);
+    f2 S;
+    if (VAR == VC) {
+        S = dt * (conv + diff);
+    } else {
+        const f2 iRe = S2((float)(1.0 / K.Re));
+        f2 bf;
+        if (VAR == VU) {
+            const f2 cval = S2(0.5f) * (ld2(A.cn, id) + ld2(A.cn, id - sx));
+            bf = alpha * (S2((float)K.FxRe) * cval - ld2(A.pg, id) * iRe);
+        } else if (VAR == VV) {
+            const f2 cval = S2(0.5f) * (ld2(A.cn, id) + ld2(A.cn, id - sy));
+            bf = alpha * (S2((float)K.FyRe) * cval - ld2(A.pg, id) * iRe);
+        } else {
+            bf = alpha * neg2(ld2(A.pg, id) * iRe);
+        }
+        S = dt * (conv + diff + bf);
+    }
+    A.S[id] = S.v.x;
+    if (live_b) A.S[id + EP_DK] = S.v.y;
+}
+
 // closure codes of the first/last unknown of an ADI line:
 // 1 b+=a (Neumann / symmetry), 2 b-=a (reflection about a wall face),
 // 3 rhs-=a*0 (Dirichlet wall face), 0 none

@@ -30,9 +30,12 @@ def test_mixed_tracks_fp64_over_200_steps():
     wl, a, b = _pair("fingering-64x32x32", 200)
     errs = {f: rel_vector(b.get, a.get, f) for f in ("c_new", "u_new", "v_new", "w_new", "phi")}
     # FP32 state rounds at ~6e-8 per operation; the fingering flow amplifies
-    # that noise, so after 200 steps c sits near 3e-6 and the velocity vector
-    # near 1e-5 of its max-norm (measured on B200)
-    assert errs["c_new"] <= 1e-5, errs
+    # that noise, so after 200 steps c sits between 1e-5 and 2.5e-5 and the
+    # velocity vector near 1e-5 of its max-norm (measured on B200; which
+    # products are fused into one rounding moves c within that band: 0.9e-5
+    # with single-cell arithmetic, 2.3e-5 with the paired FP32x2 explicit
+    # operator, both at 1.3e-7 after one step)
+    assert errs["c_new"] <= 5e-5, errs
     assert max(errs[f] for f in ("u_new", "v_new", "w_new")) <= 5e-5, errs
     assert errs["phi"] <= 1e-3, errs
     assert b.dt == pytest.approx(a.dt, rel=1e-5)
@@ -45,6 +48,17 @@ def test_mixed_routines_one_step():
     # phi is the potential of a near-cancelling divergence (FP32 velocity
     # differences lose ~3 digits); its FP32 error is ~3e-5 after one step
     assert rel_maxnorm(b.get("phi"), a.get("phi")) <= 1e-4
+
+
+def test_paired_explicit_one_step():
+    """The precision form's explicit operator computes cells (k, k+32) in
+    pairs with packed FP32x2 instructions; on 64 z cells every thread's
+    second cell is live.  One step agrees with the FP64 step to FP32 level."""
+    wl, a, b = _pair("fingering-64x64x64", 1)
+    assert b.status() == 0
+    for f in ("c_new", "u_new", "v_new", "w_new"):
+        assert rel_maxnorm(b.get(f), a.get(f)) <= 1e-4, f
+    assert rel_maxnorm(b.get("c_new"), a.get("c_new")) <= 1e-6
 
 
 @pytest.mark.parametrize("name", ["fingering-16x128x128", "fingering-8x256x256", "fingering-8x128x256"])
@@ -89,6 +103,17 @@ def test_diagnostics_match_numpy():
            + (v[3:p.nx + 3, 2:p.ny + 2, 1:p.nz + 1] - v[3:p.nx + 3, 1:p.ny + 1, 1:p.nz + 1]) / p.dy
            + (w[3:p.nx + 3, 1:p.ny + 1, 2:p.nz + 2] - w[3:p.nx + 3, 1:p.ny + 1, 1:p.nz + 1]) / p.dz)
     assert d["div_max"] == pytest.approx(np.abs(div).max(), rel=1e-9, abs=1e-12)
+
+
+def test_paired_explicit_one_step():
+    """The precision form's explicit operator computes cells (k, k+32) in
+    pairs with packed FP32x2 instructions; on 64 z cells every thread's
+    second cell is live.  One step agrees with the FP64 step to FP32 level."""
+    wl, a, b = _pair("fingering-64x64x64", 1)
+    assert b.status() == 0
+    for f in ("c_new", "u_new", "v_new", "w_new"):
+        assert rel_maxnorm(b.get(f), a.get(f)) <= 1e-4, f
+    assert rel_maxnorm(b.get("c_new"), a.get("c_new")) <= 1e-6
 
 
 @pytest.mark.parametrize("name", ["fingering-16x128x128", "fingering-8x256x256", "fingering-8x128x256"])
