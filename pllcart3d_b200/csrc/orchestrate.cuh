@@ -61,16 +61,18 @@ void launch_explicit(pllgpu_ctx* ctx, const real* un, const real* vn, const real
 }
 
 // the precision form's segmented solve along x (AXIS 0) or y (AXIS 1): lines
-// of LS_P * RS rows or one fewer, RS in {4, 8, 16, 32}; false: not applicable
-template <int VAR, int AXIS, int RS>
+// of P * RS rows or one fewer, P = 16 segments of RS in {4, 8, 16, 32} rows;
+// false: not applicable.  (32 segments of 16 rows for 512-row lines measured
+// slower: at 1024 threads a block spills its 16-row registers.)
+template <int VAR, int AXIS, int P, int RS>
 void line_seg(pllgpu_ctx* ctx, const Rng& R, const XsweepArgs<float>& X, int n)
 {
-    const dim3 grid((nk(R) + 31) / 32, AXIS == 0 ? nj(R) : ni(R)), blk(32 * LS_P);
-    constexpr size_t smem = line_seg_smem<VAR, AXIS, RS>();
-    if (n == LS_P * RS)
-        k_line_seg<VAR, AXIS, RS, true><<<grid, blk, smem, ctx->st>>>(ctx->G, R, ctx->K, X);
+    const dim3 grid((nk(R) + 31) / 32, AXIS == 0 ? nj(R) : ni(R)), blk(32 * P);
+    constexpr size_t smem = line_seg_smem<VAR, AXIS, P, RS>();
+    if (n == P * RS)
+        k_line_seg<VAR, AXIS, P, RS, true><<<grid, blk, smem, ctx->st>>>(ctx->G, R, ctx->K, X);
     else
-        k_line_seg<VAR, AXIS, RS, false><<<grid, blk, smem, ctx->st>>>(ctx->G, R, ctx->K, X);
+        k_line_seg<VAR, AXIS, P, RS, false><<<grid, blk, smem, ctx->st>>>(ctx->G, R, ctx->K, X);
 }
 
 template <int VAR, int AXIS>
@@ -78,38 +80,39 @@ bool launch_line_seg(pllgpu_ctx* ctx, const Rng& R, const XsweepArgs<float>& X)
 {
     if (ctx->P.exact_dct || ctx->nelem >= (1L << 31)) return false;
     const int n = AXIS == 0 ? ni(R) : nj(R);
-    const int rs = (n + LS_P - 1) / LS_P;   // rows per segment
+    constexpr int p = 16;
+    const int rs = (n + p - 1) / p;   // rows per segment
     if (rs != 4 && rs != 8 && rs != 16 && rs != 32) return false;
-    if (n != LS_P * rs) {
+    if (n != p * rs) {
         // one row short: the kernel loads the row past the line (and the
         // viscosity family one beyond it), which must lie in the padded box
         const int start = AXIS == 0 ? R.is : R.js, top = AXIS == 0 ? ctx->G.NX - 1 : ctx->G.NY - 1;
-        if (n != LS_P * rs - 1 || start + LS_P * rs + LineCoef<VAR, AXIS>::off > top) return false;
+        if (n != p * rs - 1 || start + p * rs + LineCoef<VAR, AXIS>::off > top) return false;
     }
-    if (rs == 4) line_seg<VAR, AXIS, 4>(ctx, R, X, n);
-    else if (rs == 8) line_seg<VAR, AXIS, 8>(ctx, R, X, n);
-    else if (rs == 16) line_seg<VAR, AXIS, 16>(ctx, R, X, n);
-    else line_seg<VAR, AXIS, 32>(ctx, R, X, n);
+    if (rs == 4) line_seg<VAR, AXIS, p, 4>(ctx, R, X, n);
+    else if (rs == 8) line_seg<VAR, AXIS, p, 8>(ctx, R, X, n);
+    else if (rs == 16) line_seg<VAR, AXIS, p, 16>(ctx, R, X, n);
+    else line_seg<VAR, AXIS, p, 32>(ctx, R, X, n);
     return true;
 }
 
-// shared-memory limits of the segmented solves (tiles pass 48 KB for RS 16
-// and 32)
-template <int VAR, int AXIS, int RS>
+// shared-memory limits of the segmented solves (the tiles pass 48 KB for
+// 16 and 32 rows per segment)
+template <int VAR, int AXIS, int P, int RS>
 void line_seg_attr()
 {
-    const int b = (int)line_seg_smem<VAR, AXIS, RS>();
-    cudaFuncSetAttribute(k_line_seg<VAR, AXIS, RS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    cudaFuncSetAttribute(k_line_seg<VAR, AXIS, RS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    const int b = (int)line_seg_smem<VAR, AXIS, P, RS>();
+    cudaFuncSetAttribute(k_line_seg<VAR, AXIS, P, RS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    cudaFuncSetAttribute(k_line_seg<VAR, AXIS, P, RS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
 }
 
 template <int VAR>
 void line_seg_attrs()
 {
-    line_seg_attr<VAR, 0, 16>();
-    line_seg_attr<VAR, 0, 32>();
-    line_seg_attr<VAR, 1, 16>();
-    line_seg_attr<VAR, 1, 32>();
+    line_seg_attr<VAR, 0, 16, 16>();
+    line_seg_attr<VAR, 0, 16, 32>();
+    line_seg_attr<VAR, 1, 16, 16>();
+    line_seg_attr<VAR, 1, 16, 32>();
 }
 
 template <typename real, int VAR>

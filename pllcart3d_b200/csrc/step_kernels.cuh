@@ -1497,12 +1497,12 @@ __global__ void __launch_bounds__(128) k_line_pf(Geo G, Rng R, Consts K, XsweepA
 // The precision form's line solve along a strided axis (x or y) by a
 // partition method: a block owns 32 neighbouring lines (lane = line, adjacent
 // k, so every row access is one coalesced 128-byte transaction) and cuts each
-// line into LS_P segments of RS rows, one warp per segment.  A thread keeps
+// line into P segments of RS rows, one warp per segment.  A thread keeps
 // its segment's right-hand side in registers; its viscosity rows (momentum)
 // and, for the x sweep, its q_old rows are copied into shared memory by
 // cp.async, each thread copying and later reading only its own rows.  The
 // thread eliminates the interior rows in terms of the segment's first row
-// (its separator) and the next segment's, the LS_P separator equations of
+// (its separator) and the next segment's, the P separator equations of
 // every line are solved by one thread per line through shared memory, and
 // each thread finishes its rows with the separators known.  Every input is
 // read once from HBM and every output written once (the sequential sweep
@@ -1511,14 +1511,13 @@ __global__ void __launch_bounds__(128) k_line_pf(Geo G, Rng R, Consts K, XsweepA
 // concentration's Neumann ghosts; y: in place into S); FP32-level agreement
 // with the sequential sweep, not bitwise.
 // ---------------------------------------------------------------------------
-constexpr int LS_P = 16;   // segments per line = warps per block
 
 // dynamic shared memory of k_line_seg: the viscosity family's rows (RS + 1
 // per thread, momentum) then the x sweep's q_old rows (RS per thread)
-template <int VAR, int AXIS, int RS>
+template <int VAR, int AXIS, int P, int RS>
 constexpr size_t line_seg_smem()
 {
-    return sizeof(float) * 32 * LS_P * ((VAR != VC ? RS + 1 : 0) + (AXIS == 0 ? RS : 0));
+    return sizeof(float) * 32 * P * ((VAR != VC ? RS + 1 : 0) + (AXIS == 0 ? RS : 0));
 }
 
 __device__ __forceinline__ void ls_cp_async4(float* dst, const float* src)
@@ -1534,25 +1533,25 @@ __device__ __forceinline__ void ls_cp_async4(float* dst, const float* src)
 // for the shared-memory rows)
 __device__ __forceinline__ void ls_fresh(float& x) { asm volatile("" : "+f"(x)); }
 
-// FULL: the line has LS_P * RS rows; else LS_P * RS - 1 and the last
+// FULL: the line has P * RS rows; else P * RS - 1 and the last
 // segment's last row is an identity row (its loads read the row past the
 // line, which the host checks lies inside the padded box)
-template <int VAR, int AXIS, int RS, bool FULL>
-__global__ void __launch_bounds__(32 * LS_P) k_line_seg(Geo G, Rng R, Consts K, XsweepArgs<float> A)
+template <int VAR, int AXIS, int P, int RS, bool FULL>
+__global__ void __launch_bounds__(32 * P) k_line_seg(Geo G, Rng R, Consts K, XsweepArgs<float> A)
 {
-    __shared__ float eq[4][LS_P][32];       // separator equations
-    __shared__ float tail[3][LS_P][32];     // last interior row of each segment
-    __shared__ float sep[LS_P + 1][32];     // separator values
+    __shared__ float eq[4][P][32];       // separator equations
+    __shared__ float tail[3][P][32];     // last interior row of each segment
+    __shared__ float sep[P + 1][32];     // separator values
     extern __shared__ float ls_dyn[];       // [row][thread] tiles: viscosity, then q_old (x)
     constexpr int LO = Closure<VAR, AXIS>::lo, HI = Closure<VAR, AXIS>::hi;
     constexpr int OFF = LineCoef<VAR, AXIS>::off;
-    constexpr int TS = 32 * LS_P;
+    constexpr int TS = 32 * P;
     const int lane = threadIdx.x & 31, l = threadIdx.x >> 5;
     const int k = R.ks + blockIdx.x * 32 + lane;
     const int o = blockIdx.y;   // j (AXIS 0) or i (AXIS 1) offset
     const bool live = k <= R.ke;
-    const bool last_seg = l == LS_P - 1;
-    constexpr int n = FULL ? LS_P * RS : LS_P * RS - 1;
+    const bool last_seg = l == P - 1;
+    constexpr int n = FULL ? P * RS : P * RS - 1;
     // offsets fit in 32 bits (the host checks the field size)
     const int st = AXIS == 0 ? (int)G.sx : (int)G.sy;
     const long base = AXIS == 0 ? (long)R.is * G.sx + (long)(R.js + o) * G.sy + k
@@ -1704,24 +1703,27 @@ __global__ void __launch_bounds__(32 * LS_P) k_line_seg(Geo G, Rng R, Consts K, 
     }
     __syncthreads();
     if (l == 0) {
-        // the LS_P separator equations of this lane's line (Thomas)
-        float cp[LS_P], rp[LS_P];
+        // the P separator equations of this lane's line (Thomas); c' and
+        // the eliminated rhs replace gamma and rho in place
         float ib = __fdividef(1.0f, eq[1][0][lane]);
-        cp[0] = eq[2][0][lane] * ib;
-        rp[0] = eq[3][0][lane] * ib;
+        float cp = eq[2][0][lane] * ib, rp = eq[3][0][lane] * ib;
+        eq[2][0][lane] = cp;
+        eq[3][0][lane] = rp;
 #pragma unroll
-        for (int t = 1; t < LS_P; ++t) {
+        for (int t = 1; t < P; ++t) {
             const float al = eq[0][t][lane];
-            ib = __fdividef(1.0f, eq[1][t][lane] - al * cp[t - 1]);
-            cp[t] = eq[2][t][lane] * ib;
-            rp[t] = (eq[3][t][lane] - al * rp[t - 1]) * ib;
+            ib = __fdividef(1.0f, eq[1][t][lane] - al * cp);
+            cp = eq[2][t][lane] * ib;
+            rp = (eq[3][t][lane] - al * rp) * ib;
+            eq[2][t][lane] = cp;
+            eq[3][t][lane] = rp;
         }
-        float x = rp[LS_P - 1];
-        sep[LS_P - 1][lane] = x;
-        sep[LS_P][lane] = 0.f;
+        float x = rp;
+        sep[P - 1][lane] = x;
+        sep[P][lane] = 0.f;
 #pragma unroll
-        for (int t = LS_P - 2; t >= 0; --t) {
-            x = rp[t] - cp[t] * x;
+        for (int t = P - 2; t >= 0; --t) {
+            x = eq[3][t][lane] - eq[2][t][lane] * x;
             sep[t][lane] = x;
         }
     }
