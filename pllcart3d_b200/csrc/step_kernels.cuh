@@ -1537,7 +1537,7 @@ __device__ __forceinline__ void ls_fresh(float& x) { asm volatile("" : "+f"(x));
 // segment's last row is an identity row (its loads read the row past the
 // line, which the host checks lies inside the padded box)
 template <int VAR, int AXIS, int P, int RS, bool FULL>
-__global__ void __launch_bounds__(32 * P) k_line_seg(Geo G, Rng R, Consts K, XsweepArgs<float> A)
+__global__ void __launch_bounds__(32 * P, RS <= 16 ? 2 : 1) k_line_seg(Geo G, Rng R, Consts K, XsweepArgs<float> A)
 {
     __shared__ float eq[4][P][32];       // separator equations
     __shared__ float tail[3][P][32];     // last interior row of each segment
