@@ -469,6 +469,113 @@ __global__ void __launch_bounds__(128) k_project(Geo G, Rng Rg, Rng Ru, Rng Rv, 
     }
 }
 
+// The precision form's projection on cell pairs (k, k+32) with packed FP32x2
+// arithmetic, as k_explicit2: the same fused correction, ghosts and pressure
+// gradient as k_project, two cells per thread sharing their addresses (the
+// second cell's are the first's plus 128 bytes) and their add / multiply /
+// fma instructions.  A second cell past ke reads the slack past the arrays'
+// ends and stores nothing.  Grid: x over k in tiles of 64 (blockDim.x 32).
+template <int VAR>
+__device__ __forceinline__ f2 pg_update2(const Consts& K, const Geo& G, const float* __restrict__ phi,
+                                         const MuPtrs<float>& mu, long id, f2 fac, f2 pold)
+{
+    const long sx = G.sx, sy = G.sy;
+    const long so = VAR == VU ? sx : VAR == VV ? sy : 1;
+    const f2 ih = S2((float)(VAR == VU ? K.ihx : VAR == VV ? K.ihy : K.ihz));
+    auto gp = [&](long p) { return (ld2(phi, p) - ld2(phi, p - so)) * ih; };
+    f2 a, b, c;
+    const f2 g0 = gp(id);
+    acoef2<VAR, 0>(K, G, mu, id, a, b, c);
+    const f2 pxx = fma2(c, gp(id + sx), fma2(b, g0, a * gp(id - sx)));
+    acoef2<VAR, 1>(K, G, mu, id, a, b, c);
+    const f2 pyy = fma2(c, gp(id + sy), fma2(b, g0, a * gp(id - sy)));
+    acoef2<VAR, 2>(K, G, mu, id, a, b, c);
+    const f2 pzz = fma2(c, gp(id + 1), fma2(b, g0, a * gp(id - 1)));
+    return pold + g0 - fac * (pyy + pxx + pzz);
+}
+
+__global__ void __launch_bounds__(128) k_project2(Geo G, Rng Rg, Rng Ru, Rng Rv, Rng Rw, Consts K,
+        float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+        float* __restrict__ pgu, float* __restrict__ pgv, float* __restrict__ pgw,
+        const float* __restrict__ phi, MuPtrs<float> mu, const double* __restrict__ scal,
+        double alpha, int do_correct, int do_ghosts, int do_pg)
+{
+    const int k = Rg.ks + blockIdx.x * (2 * EP_DK) + threadIdx.x;
+    const int j = Rg.js + blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = Rg.is + blockIdx.z;
+    if (k > Rg.ke || j > Rg.je) return;
+    const int kb = k + EP_DK;
+    const bool live_b = kb <= Rg.ke;
+    const long sx = G.sx, sy = G.sy;
+    const long id = (long)i * sx + (long)j * sy + k;
+    const double dt = scal[S_DT];
+    // per cell: in the u / v / w ranges (the second cell's k is past every ks)
+    const bool iu = (i >= Ru.is) & (i <= Ru.ie) & (j >= Ru.js);
+    const bool iv = (i <= Rv.ie) & (j >= Rv.js), iw = (i <= Rw.ie) & (j >= Rw.js);
+    const bool inu_a = iu & (k >= Ru.ks), inv_a = iv & (k >= Rv.ks), inw_a = iw & (k >= Rw.ks);
+    const bool inu_b = iu & live_b, inv_b = iv & live_b, inw_b = iw & live_b;
+    const bool ghost_i = (i <= Rg.ie);
+
+    // ghost copies of one cell (k index kk, values after correction)
+    auto ghosts = [&](long c, int kk, float uval, float vval, float wval) {
+        if (kk == Rg.ks) { u[c - 1] = uval; v[c - 1] = vval; }
+        if (kk == Rg.ke) { u[c + 1] = uval; v[c + 1] = vval; }
+        if (j == Rg.js) { u[c - sy] = -uval; w[c - sy] = -wval; }
+        if (j == Rg.je) { u[c + sy] = -uval; w[c + sy] = -wval; }
+        if (i == Rg.is) { v[c - sx] = -vval; w[c - sx] = -wval; }
+    };
+
+    if (do_correct) {
+        const f2 fac = S2((float)(dt * alpha / K.Re));
+        f2 uval = ld2(u, id), vval = S2(0.f), wval = S2(0.f);
+        if (ghost_i) {
+            vval = ld2(v, id);
+            wval = ld2(w, id);
+        }
+        const f2 p0 = ld2(phi, id);
+        const f2 vn = vval - fac * ((p0 - ld2(phi, id - sy)) * S2((float)K.ihy));
+        const f2 wn = wval - fac * ((p0 - ld2(phi, id - 1)) * S2((float)K.ihz));
+        const f2 un = uval - fac * ((p0 - ld2(phi, id - sx)) * S2((float)K.ihx));
+        if (inv_a) { v[id] = vn.v.x; vval.v.x = vn.v.x; }
+        if (inv_b) { v[id + EP_DK] = vn.v.y; vval.v.y = vn.v.y; }
+        if (inw_a) { w[id] = wn.v.x; wval.v.x = wn.v.x; }
+        if (inw_b) { w[id + EP_DK] = wn.v.y; wval.v.y = wn.v.y; }
+        if (inu_a) { u[id] = un.v.x; uval.v.x = un.v.x; }
+        if (inu_b) { u[id + EP_DK] = un.v.y; uval.v.y = un.v.y; }
+        if (i == Ru.ie + 1 && j >= Ru.js) {
+            const float def = (float)scal[S_DEFICIT];
+            if (k >= Ru.ks) u[id] = uval.v.x + def;
+            if (live_b) u[id + EP_DK] = uval.v.y + def;
+        }
+        if (do_ghosts && ghost_i) {
+            ghosts(id, k, uval.v.x, vval.v.x, wval.v.x);
+            if (live_b) ghosts(id + EP_DK, kb, uval.v.y, vval.v.y, wval.v.y);
+        }
+    } else if (do_ghosts && ghost_i) {
+        ghosts(id, k, u[id], v[id], w[id]);
+        if (live_b) ghosts(id + EP_DK, kb, u[id + EP_DK], v[id + EP_DK], w[id + EP_DK]);
+    }
+
+    if (do_pg) {
+        const f2 fac = S2((float)(0.5 * dt * alpha));
+        if (inv_a | inv_b) {
+            const f2 r = pg_update2<VV>(K, G, phi, mu, id, fac, ld2(pgv, id));
+            if (inv_a) pgv[id] = r.v.x;
+            if (inv_b) pgv[id + EP_DK] = r.v.y;
+        }
+        if (inu_a | inu_b) {
+            const f2 r = pg_update2<VU>(K, G, phi, mu, id, fac, ld2(pgu, id));
+            if (inu_a) pgu[id] = r.v.x;
+            if (inu_b) pgu[id + EP_DK] = r.v.y;
+        }
+        if (inw_a | inw_b) {
+            const f2 r = pg_update2<VW>(K, G, phi, mu, id, fac, ld2(pgw, id));
+            if (inw_a) pgw[id] = r.v.x;
+            if (inw_b) pgw[id + EP_DK] = r.v.y;
+        }
+    }
+}
+
 // slope_parameter (pllcart3d.c:722-840) on one rank: bisection for the
 // non-monotonic viscosity law's cm from c along the x line closest to
 // y=0, z=0; also leaves the law's coefficients (L895-900) in the scalars.

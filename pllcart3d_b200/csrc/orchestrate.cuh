@@ -311,6 +311,16 @@ void launch_project(pllgpu_ctx* ctx, double alpha, int correct, int ghosts, int 
     Bufs<real>& B = bufs<real>(ctx);
     const MuPtrs<real> mu = mu_new<real>(ctx);
     dim3 blk(32, 4);
+    if constexpr (std::is_same<real, float>::value) {
+        const dim3 grid((nk(ctx->Rg) + 2 * EP_DK - 1) / (2 * EP_DK), (nj(ctx->Rg) + blk.y - 1) / blk.y,
+                        ni(ctx->Rg) + 1);
+        k_project2<<<grid, blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->Rv[VU], ctx->Rv[VV], ctx->Rv[VW], ctx->K,
+                                              q_new<real>(ctx, VU), q_new<real>(ctx, VV), q_new<real>(ctx, VW),
+                                              B.pg[VU], B.pg[VV], B.pg[VW], B.phi, mu, ctx->scal, alpha, correct,
+                                              ghosts, pgu);
+        mark(ctx, "project");
+        return;
+    }
     k_project<real><<<box_grid(nk(ctx->Rg), nj(ctx->Rg), (ni(ctx->Rg) + 1 + PROJECT_NI - 1) / PROJECT_NI, blk),
                       blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->Rv[VU], ctx->Rv[VV], ctx->Rv[VW], ctx->K,
                                          q_new<real>(ctx, VU), q_new<real>(ctx, VV), q_new<real>(ctx, VW),
