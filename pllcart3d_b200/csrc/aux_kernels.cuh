@@ -73,6 +73,61 @@ __global__ void __launch_bounds__(128) k_viscosity(Geo G, Rng R, Consts K, int n
     }
 }
 
+// The precision form's exponential law on cell pairs (k, k+32) with packed
+// FP32x2 arithmetic (the averages and exponents; __expf per value), walking
+// VISC_NI planes as k_viscosity.  A second cell past NZ reads the slack past
+// the array and stores nothing.  Grid: x over k in tiles of 64.
+__global__ void __launch_bounds__(128) k_viscosity2(Geo G, Rng R, Consts K, const float* __restrict__ cn,
+                                                    float* __restrict__ mc, float* __restrict__ mxy,
+                                                    float* __restrict__ mxz, float* __restrict__ myz)
+{
+    const int k = blockIdx.x * (2 * EP_DK) + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (k >= G.NZ || j >= G.NY) return;
+    const int kb = k + EP_DK;
+    const bool live_b = kb < G.NZ;
+    const long sx = G.sx, sy = G.sy;
+    const int i0 = R.is - 1 + blockIdx.z * VISC_NI;
+    const bool jxy = (j >= R.js) & (j <= R.je + 1), jin = (j >= R.js) & (j <= R.je);
+    const bool kin_a = (k >= R.ks) & (k <= R.ke), kxz_a = (k >= R.ks) & (k <= R.ke + 1);
+    const bool kin_b = live_b & (kb <= R.ke), kxz_b = live_b & (kb <= R.ke + 1);
+    const f2 q = S2(0.25f), M = S2((float)K.M), Vn = S2((float)K.Vnorm);
+    auto law = [&](f2 c) {
+        const f2 t = M * (c - Vn);
+        return F2(__expf(t.v.x), __expf(t.v.y));
+    };
+    long id = (long)i0 * sx + (long)j * sy + k;
+    f2 p0 = ld2(cn, id - sx), py = ld2(cn, id - sx - sy), pz = ld2(cn, id - sx - 1);
+#pragma unroll
+    for (int t = 0; t < VISC_NI; ++t, id += sx) {
+        const int i = i0 + t;
+        if (i > R.ie + 1) break;
+        const f2 c0 = ld2(cn, id), cy = ld2(cn, id - sy), cz = ld2(cn, id - 1), cyz = ld2(cn, id - sy - 1);
+        const f2 vc = law(c0);
+        mc[id] = vc.v.x;
+        if (live_b) mc[id + EP_DK] = vc.v.y;
+        const bool in_i = (i >= R.is), in_i2 = (i <= R.ie);
+        if (in_i & jxy) {
+            const f2 v = law(q * (py + cy + p0 + c0));
+            if (kin_a) mxy[id] = v.v.x;
+            if (kin_b) mxy[id + EP_DK] = v.v.y;
+        }
+        if (in_i & jin) {
+            const f2 v = law(q * (pz + cz + p0 + c0));
+            if (kxz_a) mxz[id] = v.v.x;
+            if (kxz_b) mxz[id + EP_DK] = v.v.y;
+        }
+        if (in_i & in_i2 & jxy) {
+            const f2 v = law(q * (cyz + cz + cy + c0));
+            if (kxz_a) myz[id] = v.v.x;
+            if (kxz_b) myz[id + EP_DK] = v.v.y;
+        }
+        p0 = c0;
+        py = cy;
+        pz = cz;
+    }
+}
+
 // find_cfl (pllcart3d.c:3095-3118): max over interior cells of
 // |u|/dx+|v|/dy+|w|/dz at cell centres, reduced exactly through the bit
 // pattern of non-negative doubles; a NaN/Inf raises ST_NAN (the reference's

@@ -177,6 +177,16 @@ template <typename real>
 void launch_viscosity(pllgpu_ctx* ctx, const real* cn, MuPtrs<real> m, int law = -1)
 {
     dim3 blk(32, 4);
+    if constexpr (std::is_same<real, float>::value) {
+        if ((law < 0 ? ctx->P.nmvp : law) == 0) {   // the exponential law on cell pairs
+            const dim3 grid((ctx->G.NZ + 2 * EP_DK - 1) / (2 * EP_DK), (ctx->G.NY + blk.y - 1) / blk.y,
+                            (ni(ctx->Rg) + 2 + VISC_NI - 1) / VISC_NI);
+            k_viscosity2<<<grid, blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->K, cn, (float*)m.cell, (float*)m.xy,
+                                                    (float*)m.xz, (float*)m.yz);
+            mark(ctx, "viscosity");
+            return;
+        }
+    }
     k_viscosity<real><<<box_grid(ctx->G.NZ, ctx->G.NY, (ni(ctx->Rg) + 2 + VISC_NI - 1) / VISC_NI, blk), blk, 0,
                         ctx->st>>>(
         ctx->G, ctx->Rg, ctx->K, law < 0 ? ctx->P.nmvp : law, cn, (real*)m.cell, (real*)m.xy, (real*)m.xz,
