@@ -254,6 +254,102 @@ __global__ void __launch_bounds__(512) k_flux(Geo G, Rng Ru, Consts K, const rea
     }
 }
 
+// The precision form's Poisson right-hand side (k_div_rhs mode 0) on cell
+// pairs (k, k+32) with packed FP32x2 arithmetic, each thread walking
+// DIV_NI planes with u at the next plane carried in registers.  A second
+// cell past ke reads the slack past the arrays and stores nothing.
+constexpr int DIV_NI = 4;
+
+__global__ void __launch_bounds__(128) k_div_rhs2(Geo G, Rng R, Consts K, const float* __restrict__ u,
+                                                  const float* __restrict__ v, const float* __restrict__ w,
+                                                  float* __restrict__ rhs, const double* __restrict__ scal,
+                                                  double alpha)
+{
+    const int k = R.ks + blockIdx.x * (2 * EP_DK) + threadIdx.x;
+    const int j = R.js + blockIdx.y * blockDim.y + threadIdx.y;
+    if (k > R.ke || j > R.je) return;
+    const bool live_b = k + EP_DK <= R.ke;
+    const int i0 = R.is + blockIdx.z * DIV_NI;
+    const long sx = G.sx, sy = G.sy;
+    const f2 ihx = S2((float)K.ihx), ihy = S2((float)K.ihy), ihz = S2((float)K.ihz);
+    const f2 fac = S2((float)(K.Re / (scal[S_DT] * alpha)));
+    const long nj = R.je - R.js + 1, nkk = R.ke - R.ks + 1;
+    long id = (long)i0 * sx + (long)j * sy + k;
+    f2 u0 = ld2(u, id);
+#pragma unroll
+    for (int t = 0; t < DIV_NI; ++t, id += sx) {
+        const int i = i0 + t;
+        if (i > R.ie) break;
+        const f2 u1 = ld2(u, id + sx);
+        const f2 dvx = (u1 - u0) * ihx;
+        const f2 dvy = (ld2(v, id + sy) - ld2(v, id)) * ihy;
+        const f2 dvz = (ld2(w, id + 1) - ld2(w, id)) * ihz;
+        const f2 r = fac * (dvx + dvy + dvz);
+        const long c = ((long)(i - R.is) * nj + (j - R.js)) * nkk + (k - R.ks);
+        rhs[c] = r.v.x;
+        if (live_b) rhs[c + EP_DK] = r.v.y;
+        u0 = u1;
+    }
+}
+
+// The precision form's CFL scan: cell pairs (k, k+32), CFL_NI planes per
+// thread, the per-cell speed sum in FP64 (the reciprocal spacings multiply:
+// the precision form's dt may differ from the division's in the last bit)
+// and a thread-local maximum before the warp and block reductions.  The
+// maximum itself does not depend on the order.  A second cell past ke reads
+// the slack past the arrays and is left out.
+constexpr int CFL_NI = 8;
+
+__global__ void __launch_bounds__(256) k_cfl2(Geo G, Rng R, Consts K, const float* __restrict__ u,
+                                              const float* __restrict__ v, const float* __restrict__ w, double* scal,
+                                              int* status)
+{
+    const int k = R.ks + blockIdx.x * (2 * EP_DK) + threadIdx.x;
+    const int j = R.js + blockIdx.y * blockDim.y + threadIdx.y;
+    const int i0 = R.is + blockIdx.z * CFL_NI;
+    double m = 0.0;
+    bool bad = false;
+    if (k <= R.ke && j <= R.je) {
+        const bool live_b = k + EP_DK <= R.ke;
+        const long sx = G.sx, sy = G.sy;
+        long id = (long)i0 * sx + (long)j * sy + k;
+        f2 u0 = ld2(u, id);
+#pragma unroll
+        for (int t = 0; t < CFL_NI; ++t, id += sx) {
+            if (i0 + t > R.ie) break;
+            const f2 u1 = ld2(u, id + sx), v0 = ld2(v, id), v1 = ld2(v, id + sy), w0 = ld2(w, id), w1 = ld2(w, id + 1);
+            double ca = fabs(0.5 * ((double)u0.v.x + (double)u1.v.x)) * K.ihx +
+                        fabs(0.5 * ((double)v0.v.x + (double)v1.v.x)) * K.ihy +
+                        fabs(0.5 * ((double)w0.v.x + (double)w1.v.x)) * K.ihz;
+            double cb = fabs(0.5 * ((double)u0.v.y + (double)u1.v.y)) * K.ihx +
+                        fabs(0.5 * ((double)v0.v.y + (double)v1.v.y)) * K.ihy +
+                        fabs(0.5 * ((double)w0.v.y + (double)w1.v.y)) * K.ihz;
+            if (!live_b) cb = 0.0;
+            if (isfinite(ca)) m = fmax(m, ca);
+            else bad = true;
+            if (isfinite(cb)) m = fmax(m, cb);
+            else bad = true;
+            u0 = u1;
+        }
+    }
+    if (bad) atomicOr(status, (int)ST_NAN);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ double sm[8];
+    const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+    const int warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
+    if (lane == 0) sm[warp] = m;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x * blockDim.y) >> 5;
+        m = lane < nw ? sm[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0 && m > 0.0)
+            atomicMax((unsigned long long*)(scal + S_CFLMAX), (unsigned long long)__double_as_longlong(m));
+    }
+}
+
 // divergence (pllcart3d.c:1983-1999) scaled by Re/(dt alpha)
 // (phisolver_dct L2010-2024) into the compact [x][y][z] Poisson buffer.
 // With `div_out` set, the unscaled divergence also goes to the padded field.

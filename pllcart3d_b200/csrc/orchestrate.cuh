@@ -344,6 +344,16 @@ void launch_div(pllgpu_ctx* ctx, int mode, double alpha)
 {
     Bufs<real>& B = bufs<real>(ctx);
     dim3 blk(32, 4);
+    if constexpr (std::is_same<real, float>::value) {
+        if (mode == 0) {   // the precision form's right-hand side on cell pairs
+            const dim3 grid((nk(ctx->Rg) + 2 * EP_DK - 1) / (2 * EP_DK), (nj(ctx->Rg) + blk.y - 1) / blk.y,
+                            (ni(ctx->Rg) + DIV_NI - 1) / DIV_NI);
+            k_div_rhs2<<<grid, blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->K, q_new<real>(ctx, VU), q_new<real>(ctx, VV),
+                                                  q_new<real>(ctx, VW), B.dct1, ctx->scal, alpha);
+            mark(ctx, "div_rhs");
+            return;
+        }
+    }
     k_div_rhs<real><<<box_grid(nk(ctx->Rg), nj(ctx->Rg), ni(ctx->Rg), blk), blk, 0, ctx->st>>>(
         ctx->G, ctx->Rg, ctx->K, q_new<real>(ctx, VU), q_new<real>(ctx, VV), q_new<real>(ctx, VW), B.div, B.div,
         B.dct1, ctx->scal, alpha, mode);
@@ -369,9 +379,16 @@ template <typename real>
 void launch_cfl(pllgpu_ctx* ctx)
 {
     dim3 blk(32, 8);
-    k_cfl<real><<<box_grid(nk(ctx->Rg), nj(ctx->Rg), ni(ctx->Rg), blk), blk, 0, ctx->st>>>(
-        ctx->G, ctx->Rg, ctx->K, q_old<real>(ctx, VU), q_old<real>(ctx, VV), q_old<real>(ctx, VW), ctx->scal,
-        ctx->status);
+    if constexpr (std::is_same<real, float>::value) {
+        const dim3 grid((nk(ctx->Rg) + 2 * EP_DK - 1) / (2 * EP_DK), (nj(ctx->Rg) + blk.y - 1) / blk.y,
+                        (ni(ctx->Rg) + CFL_NI - 1) / CFL_NI);
+        k_cfl2<<<grid, blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->K, q_old<real>(ctx, VU), q_old<real>(ctx, VV),
+                                          q_old<real>(ctx, VW), ctx->scal, ctx->status);
+    } else {
+        k_cfl<real><<<box_grid(nk(ctx->Rg), nj(ctx->Rg), ni(ctx->Rg), blk), blk, 0, ctx->st>>>(
+            ctx->G, ctx->Rg, ctx->K, q_old<real>(ctx, VU), q_old<real>(ctx, VV), q_old<real>(ctx, VW), ctx->scal,
+            ctx->status);
+    }
     mark(ctx, "cfl");
     k_dt<<<1, 1, 0, ctx->st>>>(ctx->K, ctx->scal);
     mark(ctx, "dt");
