@@ -179,47 +179,6 @@ static __global__ void k_dt(Consts K, double* scal)
     *(unsigned long long*)(scal + S_CFLMAX) = 0ull;
 }
 
-// bulk_velo (pllcart3d.c:3381-3398): the signed value of the first (j-major,
-// k-minor) entry of largest |u| on the face i = iend; 0 if all are 0.
-// One block.
-template <typename real>
-__global__ void __launch_bounds__(1024) k_bulk_velo(Geo G, Rng R, const real* __restrict__ u, double* scal)
-{
-    const int nyz = (R.je - R.js + 1) * (R.ke - R.ks + 1), nk = R.ke - R.ks + 1;
-    double best = 0.0;
-    int bidx = 0x7fffffff;
-    for (int t = threadIdx.x; t < nyz; t += blockDim.x) {
-        const int j = R.js + t / nk, k = R.ks + t % nk;
-        double a = fabs((double)u[(long)R.ie * G.sx + (long)j * G.sy + k]);
-        if (a > best) { best = a; bidx = t; }
-    }
-    __shared__ double sb[1024];
-    __shared__ int si[1024];
-    sb[threadIdx.x] = best;
-    si[threadIdx.x] = bidx;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) {
-            double b2 = sb[threadIdx.x + s];
-            int i2 = si[threadIdx.x + s];
-            if (b2 > sb[threadIdx.x] || (b2 == sb[threadIdx.x] && i2 < si[threadIdx.x])) {
-                sb[threadIdx.x] = b2;
-                si[threadIdx.x] = i2;
-            }
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        double vb = 0.0;
-        if (sb[0] > 0.0) {
-            const int t = si[0];
-            const int j = R.js + t / nk, k = R.ks + t % nk;
-            vb = (double)u[(long)R.ie * G.sx + (long)j * G.sy + k];
-        }
-        scal[S_VBULK] = vb;
-    }
-}
-
 // inflow/outflow trapezoid fluxes of velo_correction (pllcart3d.c:2171-2223):
 // per y row a sequential sum over z of 0.5*dz*(u_k+u_{k-1}) from k=ks+1,
 // then a sequential sum over y of 0.5*dy*(q_{j-1}+q_j) from j=js+1 (wall
@@ -347,6 +306,130 @@ __global__ void __launch_bounds__(256) k_cfl2(Geo G, Rng R, Consts K, const floa
         for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
         if (lane == 0 && m > 0.0)
             atomicMax((unsigned long long*)(scal + S_CFLMAX), (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// Last-block ticket: every block's results are written and fenced before it
+// takes a ticket; the block that takes the last one reads them all and
+// resets the counter for the next launch.
+__device__ __forceinline__ bool last_block(unsigned* ticket)
+{
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (is_last) __threadfence();
+    return is_last;
+}
+
+// The precision form's inflow/outflow fluxes: the trapezoid sums of k_flux
+// in FP64, evaluated in parallel in a fixed order (every run gives the same
+// bits): one warp per row of either plane, lane l summing the terms k =
+// ks+1+l, ks+1+l+32, ... and a fixed shuffle tree; the last block forms the
+// sum over y the same way from the row sums.  Blocks of 1024 threads.
+__global__ void __launch_bounds__(1024) k_flux3(Geo G, Rng Ru, Consts K, const float* __restrict__ u, double* red,
+                                                unsigned* ticket, double* scal)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nyr = Ru.je - Ru.js + 1;
+    const double hdz = 0.5 * K.hz, hdy = 0.5 * K.hy;
+    auto tree = [&](double x) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        return x;
+    };
+    const int r = blockIdx.x * 32 + warp;   // row of plane r / nyr
+    if (r < 2 * nyr) {
+        const int plane = r / nyr, j = Ru.js + r % nyr;
+        const long b = (long)(plane ? Ru.ie + 1 : Ru.is - 1) * G.sx + (long)j * G.sy;
+        double q = 0.0;
+        for (int k = Ru.ks + 1 + lane; k <= Ru.ke; k += 32) q += hdz * ((double)u[b + k] + (double)u[b + k - 1]);
+        q = tree(q);
+        if (lane == 0) red[plane * G.NY + j] = q;
+    }
+    if (!last_block(ticket)) return;
+    if (warp == 0) {
+        double qin = 0.0, qout = 0.0;
+        for (int j = Ru.js + 1 + lane; j <= Ru.je; j += 32) {
+            qin += hdy * (__ldcg(red + j - 1) + __ldcg(red + j));
+            qout += hdy * (__ldcg(red + G.NY + j - 1) + __ldcg(red + G.NY + j));
+        }
+        qin = tree(qin);
+        qout = tree(qout);
+        if (lane == 0) {
+            scal[S_QIN] = qin;
+            scal[S_QOUT] = qout;
+            scal[S_DEFICIT] = (qin - qout) / K.area;
+            *ticket = 0u;
+        }
+    }
+}
+
+// bulk_velo (pllcart3d.c:3381-3398): the signed value of the first (j-major,
+// k-minor) entry of largest |u| on the face i = iend; 0 if all are 0.  Over
+// BULK_BLOCKS blocks: each block reduces a strided share keeping the smallest
+// index among equal values, the last block the block partials; the result
+// does not depend on the order.
+template <typename real>
+__global__ void __launch_bounds__(1024) k_bulk2(Geo G, Rng R, const real* __restrict__ u, double* red,
+                                               unsigned* ticket, double* scal)
+{
+    const int nyz = (R.je - R.js + 1) * (R.ke - R.ks + 1), nk = R.ke - R.ks + 1;
+    double best = 0.0;
+    int bidx = 0x7fffffff;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nyz; t += gridDim.x * blockDim.x) {
+        const int j = R.js + t / nk, k = R.ks + t % nk;
+        const double a = fabs((double)u[(long)R.ie * G.sx + (long)j * G.sy + k]);
+        if (a > best) { best = a; bidx = t; }
+    }
+    auto merge = [](double& b, int& i, double b2, int i2) {
+        if (b2 > b || (b2 == b && i2 < i)) { b = b2; i = i2; }
+    };
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double b2 = __shfl_xor_sync(0xffffffffu, best, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, bidx, o);
+        merge(best, bidx, b2, i2);
+    }
+    __shared__ double sb[32];
+    __shared__ int si[32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { sb[warp] = best; si[warp] = bidx; }
+    __syncthreads();
+    double* pv = red + 2L * G.NY;
+    double* pi = pv + BULK_BLOCKS;
+    if (warp == 0) {
+        best = lane < (int)(blockDim.x >> 5) ? sb[lane] : 0.0;
+        bidx = lane < (int)(blockDim.x >> 5) ? si[lane] : 0x7fffffff;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double b2 = __shfl_xor_sync(0xffffffffu, best, o);
+            const int i2 = __shfl_xor_sync(0xffffffffu, bidx, o);
+            merge(best, bidx, b2, i2);
+        }
+        if (lane == 0) { pv[blockIdx.x] = best; pi[blockIdx.x] = (double)bidx; }
+    }
+    if (!last_block(ticket)) return;
+    if (warp == 0) {
+        best = 0.0;
+        bidx = 0x7fffffff;
+        for (int b = lane; b < (int)gridDim.x; b += 32) merge(best, bidx, __ldcg(pv + b), (int)__ldcg(pi + b));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double b2 = __shfl_xor_sync(0xffffffffu, best, o);
+            const int i2 = __shfl_xor_sync(0xffffffffu, bidx, o);
+            merge(best, bidx, b2, i2);
+        }
+        if (lane == 0) {
+            double vb = 0.0;
+            if (best > 0.0) {
+                const int j = R.js + bidx / nk, k = R.ks + bidx % nk;
+                vb = (double)u[(long)R.ie * G.sx + (long)j * G.sy + k];
+            }
+            scal[S_VBULK] = vb;
+            *ticket = 0u;
+        }
     }
 }
 

@@ -92,6 +92,12 @@ struct MuPtrs {
 // launch-shape variants the autotuner chooses among; every variant computes
 // each cell (explicit operators) or line (line solves) with the same
 // arithmetic, so the choice changes timing only, never a bit of the result
+// Scratch of the multi-block reductions: the flux row sums of both x
+// planes (2 NY) and the bulk-velocity block partials (value and index,
+// BULK_BLOCKS each).
+constexpr int BULK_BLOCKS = 128;
+inline long red_doubles(const Geo& G) { return 2L * G.NY + 2L * BULK_BLOCKS; }
+
 constexpr int NTUNE_EXP = 4, NTUNE_LINE = 3;
 inline void tune_exp_block(int v, int& bx, int& by)
 {

@@ -69,6 +69,8 @@ struct pllgpu_ctx {
     double* scal = nullptr;     // device scalars (S_*)
     int* status = nullptr;      // device sticky status bits
     double* work = nullptr;     // slope-parameter scratch
+    double* red = nullptr;      // multi-block reduction partials (RED_DOUBLES)
+    unsigned* ticket = nullptr; // last-block tickets of those reductions (2, self-resetting)
     double* diag = nullptr;     // per-plane diagnostics + results
     int cur = 0;                // buffer index holding the "old" role
     bool resync_c = false;      // after a restart: copy c's buffers once (resume)

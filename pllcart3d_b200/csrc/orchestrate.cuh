@@ -363,6 +363,13 @@ void launch_div(pllgpu_ctx* ctx, int mode, double alpha)
 template <typename real>
 void launch_flux(pllgpu_ctx* ctx)
 {
+    if constexpr (std::is_same<real, float>::value) {
+        const int rows = 2 * nj(ctx->Rv[VU]);
+        k_flux3<<<(rows + 31) / 32, 1024, 0, ctx->st>>>(ctx->G, ctx->Rv[VU], ctx->K, q_new<real>(ctx, VU), ctx->red,
+                                                        ctx->ticket, ctx->scal);
+        mark(ctx, "flux");
+        return;
+    }
     k_flux<real><<<1, 512, sizeof(double) * 2 * ctx->G.NY, ctx->st>>>(ctx->G, ctx->Rv[VU], ctx->K,
                                                                        q_new<real>(ctx, VU), ctx->scal);
     mark(ctx, "flux");
@@ -371,7 +378,8 @@ void launch_flux(pllgpu_ctx* ctx)
 template <typename real>
 void launch_bulk(pllgpu_ctx* ctx)
 {
-    k_bulk_velo<real><<<1, 1024, 0, ctx->st>>>(ctx->G, ctx->Rg, q_old<real>(ctx, VU), ctx->scal);
+    k_bulk2<real><<<BULK_BLOCKS, 1024, 0, ctx->st>>>(ctx->G, ctx->Rg, q_old<real>(ctx, VU), ctx->red,
+                                                      ctx->ticket + 1, ctx->scal);
     mark(ctx, "bulk_velo");
 }
 

@@ -228,7 +228,8 @@ pllgpu_ctx* pllgpu_create(const pllgpu_params* p, int device)
     ok = ok && (c->mode_cc = dalloc<double>(c, ncell)) && (c->mode_rr = dalloc<double>(c, ncell)) &&
          (c->lam_y = dalloc<double>(c, p->ny)) && (c->lam_z = dalloc<double>(c, p->nz)) &&
          (c->scal = dalloc<double>(c, S_COUNT)) && (c->work = dalloc<double>(c, 2L * (p->nx + 8))) &&
-         (c->diag = dalloc<double>(c, 3L * p->nx + 8)) && (c->status = dalloc<int>(c, 1));
+         (c->diag = dalloc<double>(c, 3L * p->nx + 8)) && (c->status = dalloc<int>(c, 1)) &&
+         (c->red = dalloc<double>(c, red_doubles(c->G))) && (c->ticket = dalloc<unsigned>(c, 2));
     if (ok && ctx->mixed) ok = (c->stage64 = dalloc<double>(c, c->nelem)) != nullptr;
     if (!ok) {
         pllgpu_destroy(ctx);
