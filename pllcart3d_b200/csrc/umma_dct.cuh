@@ -1,6 +1,6 @@
 // The DCT passes of the precision form on the 5th-generation tensor cores:
 // split-TF32 (3-term compensated) GEMMs issued with tcgen05.mma, operands
-// staged in shared memory by TMA (cp.async.bulk.tensor, 128-byte swizzle),
+// staged in shared memory by TMA (cp.async.bulk.tensor, 64-byte swizzle),
 // the FP32 accumulator in tensor memory and read back with tcgen05.ld.
 //
 // Every pass of the 2-d DCT-II / DCT-III over an x-plane (fftw_3d.h:45-106
@@ -23,7 +23,7 @@
 // of positions, so elementwise conversion preserves it).
 //
 // CTA: 128 rows x BN columns (BN = the whole transform length, 128 or 256),
-// K in chunks of 32 (one 128-byte swizzle row), two pipeline stages.
+// K in chunks of 16 (one 64-byte swizzle row), four pipeline stages.
 //   warp 0      TMA producer (one thread)
 //   warp 1      TMEM owner and MMA issuer (one thread)
 //   warps 2..5  converters, then the epilogue (TMEM lanes 32*(warp%4)...)
@@ -44,8 +44,8 @@ namespace pll {
 namespace {
 
 constexpr int UM_BM = 128;       // rows per CTA (tcgen05 M)
-constexpr int UM_BK = 32;        // K chunk: 32 fp32 = one 128-byte swizzle row
-constexpr int UM_STAGES = 2;
+constexpr int UM_BK = 16;        // K chunk: 16 fp32 = one 64-byte swizzle row
+constexpr int UM_STAGES = 4;
 constexpr int UM_THREADS = 192;
 constexpr long long UM_WAIT_CYCLES = 2000000000LL;   // ~1 s at 1.9 GHz
 
@@ -64,7 +64,7 @@ struct UmmaSmem {
     static constexpr uint32_t STAGE = 2 * A_BYTES + 2 * B_BYTES;
     static constexpr uint32_t BAR_OFF = UM_STAGES * STAGE;
     // full[2], conv[2], empty[2], done, then the TMEM address and abort flag
-    static constexpr uint32_t TOTAL = BAR_OFF + 128;
+    static constexpr uint32_t TOTAL = BAR_OFF + 256;
     static constexpr uint32_t DYN = TOTAL + 1024;   // slack for 1024-byte alignment
 };
 
@@ -126,16 +126,16 @@ __device__ __forceinline__ void um_tma_2d(void* dst, const CUtensorMap* map, uin
         : "memory");
 }
 
-// shared-memory matrix descriptor: K-major, 128-byte swizzle, rows of 128 B
-// packed (8-row groups 1024 B apart), descriptor version 1 (sm_100)
-__device__ __forceinline__ uint64_t um_desc_sw128(uint32_t saddr)
+// shared-memory matrix descriptor: K-major, 64-byte swizzle, rows of 64 B
+// packed (8-row groups 512 B apart), descriptor version 1 (sm_100)
+__device__ __forceinline__ uint64_t um_desc_sw64(uint32_t saddr)
 {
     uint64_t d = 0;
     d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);   // start address, bits 0-13
     d |= (uint64_t)1 << 16;                      // leading byte offset (unused here)
-    d |= (uint64_t)(1024 >> 4) << 32;            // stride byte offset, bits 32-45
+    d |= (uint64_t)(512 >> 4) << 32;             // stride byte offset, bits 32-45
     d |= (uint64_t)1 << 46;                      // version
-    d |= (uint64_t)2 << 61;                      // SWIZZLE_128B
+    d |= (uint64_t)4 << 61;                      // SWIZZLE_64B
     return d;
 }
 
@@ -199,12 +199,12 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
     extern __shared__ uint8_t um_raw[];
     uint8_t* sm = (uint8_t*)(((uintptr_t)um_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* bars = (uint64_t*)(sm + L::BAR_OFF);
-    uint64_t* full = bars;        // TMA landed (A fp32, T hi, T lo)
-    uint64_t* conv = bars + 2;    // A split into hi / lo
-    uint64_t* empty = bars + 4;   // MMAs of the stage retired
-    uint64_t* done = bars + 6;    // accumulator complete
-    volatile uint32_t* tmem_slot = (volatile uint32_t*)(bars + 7);
-    volatile int* abort_flag = (volatile int*)(bars + 8);
+    uint64_t* full = bars;                    // TMA landed (A fp32, T hi, T lo)
+    uint64_t* conv = bars + UM_STAGES;        // A split into hi / lo
+    uint64_t* empty = bars + 2 * UM_STAGES;   // MMAs of the stage retired
+    uint64_t* done = bars + 3 * UM_STAGES;    // accumulator complete
+    volatile uint32_t* tmem_slot = (volatile uint32_t*)(bars + 3 * UM_STAGES + 1);
+    volatile int* abort_flag = (volatile int*)(bars + 3 * UM_STAGES + 2);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * UM_BM;
@@ -234,10 +234,12 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
 
     if (warp == 0) {
         if (lane == 0) {
-            int last[UM_STAGES] = {-1, -1};
+            int last[UM_STAGES];
+#pragma unroll
+            for (int s = 0; s < UM_STAGES; ++s) last[s] = -1;
             for (int kc = 0; kc < nk; ++kc) {
-                const int s = kc & 1;
-                if (kc >= UM_STAGES && !um_wait(&empty[s], ((kc >> 1) + 1) & 1, abort_flag, true)) break;
+                const int s = kc % UM_STAGES;
+                if (kc >= UM_STAGES && !um_wait(&empty[s], (kc / UM_STAGES + 1) & 1, abort_flag, true)) break;
                 uint8_t* st = sm + s * L::STAGE;
                 um_arrive_tx(&full[s], L::A_BYTES + 2 * L::B_BYTES);
                 um_tma_2d(st, &tmA, &full[s], kc * UM_BK, m0);
@@ -247,21 +249,21 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
             }
             // drain: no copy may still be landing when the CTA leaves
             for (int s = 0; s < UM_STAGES; ++s)
-                if (last[s] >= 0) um_wait(&full[s], (last[s] >> 1) & 1, abort_flag, false);
+                if (last[s] >= 0) um_wait(&full[s], (last[s] / UM_STAGES) & 1, abort_flag, false);
         }
         __syncwarp();
     } else if (warp == 1) {
         if (lane == 0) {
             const uint32_t idesc = um_idesc_tf32<BN>();
             for (int kc = 0; kc < nk; ++kc) {
-                const int s = kc & 1;
-                if (!um_wait(&conv[s], (kc >> 1) & 1, abort_flag, true)) break;
+                const int s = kc % UM_STAGES;
+                if (!um_wait(&conv[s], (kc / UM_STAGES) & 1, abort_flag, true)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                 const uint32_t st = um_smem(sm + s * L::STAGE);
-                const uint64_t dh = um_desc_sw128(st);
-                const uint64_t dl = um_desc_sw128(st + L::A_BYTES);
-                const uint64_t bh = um_desc_sw128(st + 2 * L::A_BYTES);
-                const uint64_t bl = um_desc_sw128(st + 2 * L::A_BYTES + L::B_BYTES);
+                const uint64_t dh = um_desc_sw64(st);
+                const uint64_t dl = um_desc_sw64(st + L::A_BYTES);
+                const uint64_t bh = um_desc_sw64(st + 2 * L::A_BYTES);
+                const uint64_t bl = um_desc_sw64(st + 2 * L::A_BYTES + L::B_BYTES);
 #pragma unroll
                 for (int kk = 0; kk < UM_BK / 8; ++kk) {
                     // K step of 8 tf32 = 32 bytes inside the swizzle row
@@ -279,8 +281,8 @@ __global__ void __launch_bounds__(UM_THREADS, 1)
     } else {
         const int ct = threadIdx.x - 64;   // 0..127
         for (int kc = 0; kc < nk; ++kc) {
-            const int s = kc & 1;
-            if (!um_wait(&full[s], (kc >> 1) & 1, abort_flag, true)) break;
+            const int s = kc % UM_STAGES;
+            if (!um_wait(&full[s], (kc / UM_STAGES) & 1, abort_flag, true)) break;
             float4* a = (float4*)(sm + s * L::STAGE);
             float4* lo = (float4*)(sm + s * L::STAGE + L::A_BYTES);
 #pragma unroll 4
@@ -373,7 +375,7 @@ struct UmmaPSmem {
     static constexpr uint32_t EPI_OFF = UM_STAGES * STAGE;            // 4 x 32x33 floats
     static constexpr uint32_t BAR_OFF = EPI_OFF + 4 * 32 * 33 * 4;
     // full[2] conv[2] empty[2] tfull[2] tempty[2] done, TMEM address, abort
-    static constexpr uint32_t TOTAL = BAR_OFF + 128;
+    static constexpr uint32_t TOTAL = BAR_OFF + 256;
     static constexpr uint32_t DYN = TOTAL + 1024;
 };
 
@@ -388,13 +390,13 @@ __global__ void __launch_bounds__(UMP_THREADS, 1)
     uint8_t* sm = (uint8_t*)(((uintptr_t)ump_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* bars = (uint64_t*)(sm + L::BAR_OFF);
     uint64_t* full = bars;
-    uint64_t* conv = bars + 2;
-    uint64_t* empty = bars + 4;
-    uint64_t* tfull = bars + 6;
-    uint64_t* tempty = bars + 8;
-    uint64_t* done = bars + 10;
-    volatile uint32_t* tmem_slot = (volatile uint32_t*)(bars + 11);
-    volatile int* abort_flag = (volatile int*)(bars + 12);
+    uint64_t* conv = bars + UM_STAGES;
+    uint64_t* empty = bars + 2 * UM_STAGES;
+    uint64_t* tfull = bars + 3 * UM_STAGES;
+    uint64_t* tempty = bars + 3 * UM_STAGES + 2;
+    uint64_t* done = bars + 3 * UM_STAGES + 4;
+    volatile uint32_t* tmem_slot = (volatile uint32_t*)(bars + 3 * UM_STAGES + 5);
+    volatile int* abort_flag = (volatile int*)(bars + 3 * UM_STAGES + 6);
     constexpr uint32_t TCOLS = 2 * BN;   // two accumulators
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -431,11 +433,13 @@ __global__ void __launch_bounds__(UMP_THREADS, 1)
 
     if (warp == 0) {
         if (lane == 0) {
-            int last[UM_STAGES] = {-1, -1};
+            int last[UM_STAGES];
+#pragma unroll
+            for (int s = 0; s < UM_STAGES; ++s) last[s] = -1;
             for (int g = 0; g < total; ++g) {
-                const int s = g & 1, kc = g % nk;
+                const int s = g % UM_STAGES, kc = g % nk;
                 const int m0 = ((int)blockIdx.x + (g / nk) * (int)gridDim.x) * UM_BM;
-                if (g >= UM_STAGES && !um_wait(&empty[s], ((g >> 1) + 1) & 1, abort_flag, true)) break;
+                if (g >= UM_STAGES && !um_wait(&empty[s], (g / UM_STAGES + 1) & 1, abort_flag, true)) break;
                 uint8_t* st = sm + s * L::STAGE;
                 um_arrive_tx(&full[s], L::A_BYTES + 2 * L::B_BYTES);
                 um_tma_2d(st, &tmA, &full[s], kc * UM_BK, m0);
@@ -444,7 +448,7 @@ __global__ void __launch_bounds__(UMP_THREADS, 1)
                 last[s] = g;
             }
             for (int s = 0; s < UM_STAGES; ++s)
-                if (last[s] >= 0) um_wait(&full[s], (last[s] >> 1) & 1, abort_flag, false);
+                if (last[s] >= 0) um_wait(&full[s], (last[s] / UM_STAGES) & 1, abort_flag, false);
         }
         __syncwarp();
     } else if (warp == 1) {
@@ -457,17 +461,17 @@ __global__ void __launch_bounds__(UMP_THREADS, 1)
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                 const uint32_t acc = tmem + (uint32_t)(a * BN);
                 for (int kc = 0; kc < nk; ++kc) {
-                    const int g = it * nk + kc, s = g & 1;
-                    if (!um_wait(&conv[s], (g >> 1) & 1, abort_flag, true)) {
+                    const int g = it * nk + kc, s = g % UM_STAGES;
+                    if (!um_wait(&conv[s], (g / UM_STAGES) & 1, abort_flag, true)) {
                         ok = false;
                         break;
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                     const uint32_t st = um_smem(sm + s * L::STAGE);
-                    const uint64_t dh = um_desc_sw128(st);
-                    const uint64_t dl = um_desc_sw128(st + L::A_BYTES);
-                    const uint64_t bh = um_desc_sw128(st + 2 * L::A_BYTES);
-                    const uint64_t bl = um_desc_sw128(st + 2 * L::A_BYTES + L::B_BYTES);
+                    const uint64_t dh = um_desc_sw64(st);
+                    const uint64_t dl = um_desc_sw64(st + L::A_BYTES);
+                    const uint64_t bh = um_desc_sw64(st + 2 * L::A_BYTES);
+                    const uint64_t bl = um_desc_sw64(st + 2 * L::A_BYTES + L::B_BYTES);
 #pragma unroll
                     for (int kk = 0; kk < UM_BK / 8; ++kk) {
                         const uint64_t o = (uint64_t)(kk * 32) >> 4;
@@ -485,8 +489,8 @@ __global__ void __launch_bounds__(UMP_THREADS, 1)
     } else if (warp < 6) {
         const int ct = threadIdx.x - 64;   // 0..127
         for (int g = 0; g < total; ++g) {
-            const int s = g & 1;
-            if (!um_wait(&full[s], (g >> 1) & 1, abort_flag, true)) break;
+            const int s = g % UM_STAGES;
+            if (!um_wait(&full[s], (g / UM_STAGES) & 1, abort_flag, true)) break;
             float4* a = (float4*)(sm + s * L::STAGE);
             float4* lo = (float4*)(sm + s * L::STAGE + L::A_BYTES);
 #pragma unroll 4
