@@ -810,6 +810,92 @@ __global__ void __launch_bounds__(128) k_project2(Geo G, Rng Rg, Rng Ru, Rng Rv,
     }
 }
 
+// The precision form's mode solve with a third of k_poisson_x's scratch
+// traffic: the same FP64 Thomas recurrences per (ky, kz) mode, but the
+// eliminated right-hand side is kept in FP32 (the mode data are FP32 on
+// either side of the solve) and c' is not stored: it depends on the mode
+// only, so the forward sweep records it every PX_CK rows and the backward
+// sweep recomputes each block of PX_CK values from its checkpoint (the same
+// arithmetic, so the same values).  One reciprocal per row and sweep instead
+// of two divisions.  16.5 bytes per cell instead of 40.
+constexpr int PX_CK = 16;
+
+__global__ void __launch_bounds__(128) k_poisson_x2(int nx, int ny, int nz, Consts K,
+                                                    const double* __restrict__ lam_y,
+                                                    const double* __restrict__ lam_z, float* __restrict__ hat,
+                                                    float* __restrict__ rr, double* __restrict__ ck, int kz_major)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int N = ny * nz;
+    if (t >= N) return;
+    const int jy = kz_major ? t % ny : t / nz, kz = kz_major ? t / ny : t % nz;
+    const long st = N;
+    const double a = K.dx2i, c = K.dx2i;
+    const double bmid = -2.0 * K.dx2i + lam_y[jy] + lam_z[kz];
+    const bool gauge = (jy == 0) && (kz == 0);
+    auto diag = [&](int m) {
+        double lb = bmid;
+        if (m == 0) lb += a;
+        if (m == nx - 1 && !gauge) lb += c;
+        return lb;
+    };
+    // forward: c'_m = c / (b_m - a c'_{m-1}), r'_m = (r_m - a r'_{m-1}) / (...)
+    constexpr int PF = 8;
+    double cprev = 0.0, rprev = 0.0;
+    float hv[PF];
+#pragma unroll
+    for (int u = 0; u < PF; ++u) hv[u] = u < nx ? hat[t + (long)u * st] : 0.f;
+    for (int m0 = 0; m0 < nx; m0 += PF) {
+        float hn[PF];
+#pragma unroll
+        for (int u = 0; u < PF; ++u) {
+            const int m = m0 + PF + u;
+            hn[u] = m < nx ? hat[t + (long)m * st] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < PF; ++u) {
+            const int m = m0 + u;
+            if (m < nx) {
+                if (m % PX_CK == 0) ck[(long)(m / PX_CK) * st + t] = cprev;   // c'_{m-1}
+                const double inv = 1.0 / (diag(m) - cprev * a);
+                const double rm = ((double)hv[u] - rprev * a) * inv;
+                cprev = c * inv;   // as the backward sweep recomputes it
+                rprev = rm;
+                rr[t + (long)m * st] = (float)rm;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < PF; ++u) hv[u] = hn[u];
+    }
+    // backward, one checkpoint block at a time from the end: x_{n-1} = r'_{n-1}
+    double xnext = 0.0;
+    for (int b0 = ((nx - 1) / PX_CK) * PX_CK; b0 >= 0; b0 -= PX_CK) {
+        double cb[PX_CK];
+        float rv[PX_CK];
+        double cp = ck[(long)(b0 / PX_CK) * st + t];
+#pragma unroll
+        for (int u = 0; u < PX_CK; ++u) {
+            const int m = b0 + u;
+            rv[u] = m < nx ? rr[t + (long)m * st] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < PX_CK; ++u) {
+            const int m = b0 + u;
+            if (m < nx) cp = c * (1.0 / (diag(m) - cp * a));
+            cb[u] = cp;
+        }
+#pragma unroll
+        for (int u = PX_CK - 1; u >= 0; --u) {
+            const int m = b0 + u;
+            if (m < nx) {
+                const double x = (m == nx - 1) ? (double)rv[u] : (double)rv[u] - cb[u] * xnext;
+                hat[t + (long)m * st] = (float)x;
+                xnext = x;
+            }
+        }
+    }
+}
+
 // slope_parameter (pllcart3d.c:722-840) on one rank: bisection for the
 // non-monotonic viscosity law's cm from c along the x line closest to
 // y=0, z=0; also leaves the law's coefficients (L895-900) in the scalars.

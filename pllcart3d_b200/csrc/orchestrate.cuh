@@ -254,8 +254,8 @@ void launch_poisson_umma(pllgpu_ctx* ctx)
     launch_umma(ctx, 0, (long)nx * ny, nz, UmmaEpi{ny, N, 1, ny, 1.f, 0, 1}, B.dct2);
     // forward y: dct1[x][kz][ky] = sum_y dct2[x][kz][y] Ty[ky][y]
     launch_umma(ctx, 1, (long)nx * nz, ny, UmmaEpi{nz, N, ny, 1, 1.f, 0, 0}, B.dct1);
-    k_poisson_x<float><<<(int)((N + 127) / 128), 128, 0, ctx->st>>>(nx, ny, nz, ctx->K, ctx->lam_y, ctx->lam_z,
-                                                                   B.dct1, ctx->mode_cc, ctx->mode_rr, 1);
+    k_poisson_x2<<<(int)((N + 127) / 128), 128, 0, ctx->st>>>(nx, ny, nz, ctx->K, ctx->lam_y, ctx->lam_z, B.dct1,
+                                                             (float*)ctx->mode_rr, ctx->mode_cc, 1);
     mark(ctx, "poisson_x");
     // inverse y: dct2[x][y][kz] = sum_ky dct1[x][kz][ky] Tiy[y][ky] (stored transposed)
     launch_umma(ctx, 2, (long)nx * nz, ny, UmmaEpi{nz, N, 1, nz, 1.f, 0, 1}, B.dct2);
