@@ -728,7 +728,7 @@ __device__ __forceinline__ f2 pg_update2(const Consts& K, const Geo& G, const fl
     return pold + g0 - fac * (pyy + pxx + pzz);
 }
 
-__global__ void __launch_bounds__(128) k_project2(Geo G, Rng Rg, Rng Ru, Rng Rv, Rng Rw, Consts K,
+__global__ void __launch_bounds__(128, 16) k_project2(Geo G, Rng Rg, Rng Ru, Rng Rv, Rng Rw, Consts K,
         float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
         float* __restrict__ pgu, float* __restrict__ pgv, float* __restrict__ pgw,
         const float* __restrict__ phi, MuPtrs<float> mu, const double* __restrict__ scal,

@@ -543,7 +543,7 @@ __device__ __forceinline__ void acoef2(const Consts& K, const Geo& G, const MuPt
 
 // grid: x over k in tiles of 2 * EP_DK (blockDim.x == EP_DK), y over j, z over i
 template <int VAR>
-__global__ void __launch_bounds__(128, 12) k_explicit2(Geo G, Rng R, Consts K, ExplicitArgs<float> A)
+__global__ void __launch_bounds__(128, 16) k_explicit2(Geo G, Rng R, Consts K, ExplicitArgs<float> A)
 {
     const int k = R.ks + blockIdx.x * (2 * EP_DK) + threadIdx.x;
     const int j = R.js + blockIdx.y * blockDim.y + threadIdx.y;
