@@ -50,6 +50,27 @@ FAMILY = {
     "dct_umma": "k_dct_umma", "poisson_x": "k_poisson_x", "project": "k_project", "cfl": "k_cfl",
 }
 
+# the precision form's kernels where they differ from the FP64 form's
+FAMILY_FP32 = {
+    "explicit_c": "k_explicit2", "explicit_u": "k_explicit2", "explicit_v": "k_explicit2",
+    "explicit_w": "k_explicit2",
+    "adi_y_c": "k_line_seg (y)", "adi_y_u": "k_line_seg (y)", "adi_y_v": "k_line_seg (y)",
+    "adi_y_w": "k_line_seg (y)",
+    "adi_z_c": "k_adi_z_part", "adi_z_u": "k_adi_z_part", "adi_z_v": "k_adi_z_part", "adi_z_w": "k_adi_z_part",
+    "adi_x_c": "k_line_seg (x)", "adi_x_u": "k_line_seg (x)", "adi_x_v": "k_line_seg (x)",
+    "adi_x_w": "k_line_seg (x)",
+    "viscosity": "k_viscosity2", "div_rhs": "k_div_rhs2", "dct_umma": "k_dct_umma_p",
+    "poisson_x": "k_poisson_x2", "project": "k_project2", "cfl": "k_cfl2",
+}
+
+
+def family(label: str, precision: str = "fp64"):
+    """Kernel (family) that runs `label` in the given form, or None."""
+    if precision == "fp32" and label in FAMILY_FP32:
+        return FAMILY_FP32[label]
+    return FAMILY.get(label)
+
+
 # tensor-core kernels: products per DCT pass (one dense product of 2 n flops
 # per cell for a pass of length n; the precision form's split-TF32 passes
 # issue 3: hi*hi, hi*lo, lo*hi)
