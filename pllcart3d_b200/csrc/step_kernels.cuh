@@ -637,77 +637,6 @@ struct Closure {
     static constexpr int hi = AXIS == 0 ? 0 : lo;
 };
 
-// ---------------------------------------------------------------------------
-// ADI line solve along y or z: (1 - fac A) x = S, serial Thomas as
-// tridiag_1rhs (pllcart3d.c:3511-3536); one thread per line; the eliminated
-// c' goes to scratch `cc`, the eliminated rhs overwrites S in place
-// (concentration L592-650, xmom L991-1049, ymom L1148-1206, zmom L1300-1354)
-// ---------------------------------------------------------------------------
-template <int VAR, int AXIS, typename real>
-__global__ void __launch_bounds__(128) k_adi_yz(Geo G, Rng R, Consts K, MuPtrs<real> mu,
-                                                real* __restrict__ S, real* __restrict__ cc,
-                                                const double* __restrict__ scal, double alpha)
-{
-    // line index: AXIS==1 -> (i, k); AXIS==2 -> (i, j)
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = R.is + blockIdx.y;
-    int j, k;
-    long st;
-    int n;
-    if (AXIS == 1) {
-        k = R.ks + t;
-        if (k > R.ke) return;
-        j = R.js;
-        st = G.sy;
-        n = R.je - R.js + 1;
-    } else {
-        j = R.js + t;
-        if (j > R.je) return;
-        k = R.ks;
-        st = 1;
-        n = R.ke - R.ks + 1;
-    }
-    const real fac = (real)(0.5 * scal[S_DT] * alpha);
-    const long base = (long)i * G.sx + (long)j * G.sy + k;
-    constexpr int LO = Closure<VAR, AXIS>::lo, HI = Closure<VAR, AXIS>::hi;
-    real cprev = 0, rprev = 0;
-    for (int m = 0; m < n; ++m) {
-        const long id = base + (long)m * st;
-        real a, b, c;
-        acoef<VAR, AXIS, real>(K, G, mu.cell, mu.xy, mu.xz, mu.yz, id, a, b, c);
-        real la = -fac * a, lb = (real)1.0 - fac * b, lc = -fac * c, lr = S[id];
-        if (m == 0) {
-            if (LO == 1) lb += la;
-            else if (LO == 2) lb -= la;
-            else if (LO == 3) lr -= la * (real)0.0;
-        }
-        if (m == n - 1) {
-            if (HI == 1) lb += lc;
-            else if (HI == 2) lb -= lc;
-            else if (HI == 3) lr -= lc * (real)0.0;
-        }
-        real bb, cm, rm;
-        if (m == 0) {
-            bb = lb;
-            thomas_div<real>(lc, lr, bb, cm, rm);
-        } else {
-            bb = lb - cprev * la;
-            thomas_div<real>(lc, (lr - rprev * la), bb, cm, rm);
-        }
-        cc[id] = cm;
-        S[id] = rm;
-        cprev = cm;
-        rprev = rm;
-    }
-    real xnext = rprev;
-    for (int m = n - 2; m >= 0; --m) {
-        const long id = base + (long)m * st;
-        real x = S[id] - xnext * cc[id];
-        S[id] = x;
-        xnext = x;
-    }
-}
-
 template <typename real>
 struct XsweepArgs {
     MuPtrs<real> mu;     // mu_new
@@ -722,103 +651,12 @@ struct XsweepArgs {
 };
 
 // ---------------------------------------------------------------------------
-// ADI line solve along x with pll_tridiag's one-rank arithmetic
-// (pll_tridiag.c:21-47, 96-110), the convective outflow closure
-// (e.g. pllcart3d.c:677-683), new = old + delta, and for c the Neumann
-// ghost copies of pllcart3d.c:700-712.  One thread per (j,k) line.
-// ---------------------------------------------------------------------------
-template <int VAR, typename real>
-__global__ void __launch_bounds__(128) k_adi_x(Geo G, Rng R, Consts K, XsweepArgs<real> A)
-{
-    const int k = R.ks + blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = R.js + blockIdx.y;
-    if (k > R.ke) return;
-    const long sx = G.sx;
-    const int n = R.ie - R.is + 1;
-    const real dt = (real)A.scal[S_DT];
-    const real fac = (real)(0.5 * A.scal[S_DT] * A.alpha);
-    const real vbulk = (real)A.scal[S_VBULK];
-    const long base = (long)R.is * sx + (long)j * G.sy + k;
-    const long rb = base + (long)n * sx;
-    constexpr int LO = Closure<VAR, 0>::lo;
-    // outflow plane, explicit convective boundary condition
-    real Hb = -vbulk * (A.q[rb] - A.q[rb - sx]);
-    Hb = over_h<real>(Hb, K.hx, K.ihx, K.pow2);
-    A.H[rb] = Hb;
-    const real boun = dt * ((real)A.g * Hb + (real)A.r * A.Hm[rb]);
-    A.qn[rb] = A.q[rb] + boun;
-
-    real cprev = 0, rprev = 0;
-    for (int m = 0; m < n; ++m) {
-        const long id = base + (long)m * sx;
-        real a, b, c;
-        acoef<VAR, 0, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
-        real la = -fac * a, lb = (real)1.0 - fac * b, lc = -fac * c, lr = A.S[id];
-        if (m == 0) {
-            if (LO == 2) lb -= la;
-            else if (LO == 3) lr -= la * (real)0.0;
-        }
-        if (m == n - 1) lr -= lc * boun;
-        real cm, rm;
-        if (m == 0) {
-            lb = lb - (real)0.0 * la;
-            thomas_div<real>(lc, (lr - (real)0.0 * la), lb, cm, rm);
-        } else {
-            lb = (lb - cprev * la);
-            thomas_div<real>(lc, (lr - rprev * la), lb, cm, rm);
-        }
-        A.cc[id] = cm;
-        A.S[id] = rm;
-        cprev = cm;
-        rprev = rm;
-    }
-    // back substitution, q_new = q_old + delta
-    real xnext = rprev - cprev * (real)0.0;
-    {
-        const long id = base + (long)(n - 1) * sx;
-        A.qn[id] = A.q[id] + xnext;
-    }
-    for (int m = n - 2; m >= 0; --m) {
-        const long id = base + (long)m * sx;
-        real x = A.S[id] - A.cc[id] * xnext;
-        A.qn[id] = A.q[id] + x;
-        xnext = x;
-    }
-    if (VAR == VC) {
-        // Neumann ghosts in y (pllcart3d.c:700-705) then z (L707-712); the
-        // z copies run over j in [js-1, je+1] so the corners copy the y
-        // ghosts, which equal this line's values
-        const long sy = G.sy;
-        const bool jlo = (j == R.js), jhi = (j == R.je);
-        const bool klo = (k == R.ks), khi = (k == R.ke);
-        if (jlo | jhi | klo | khi) {
-            for (int m = 0; m < n; ++m) {
-                const long id = base + (long)m * sx;
-                const real v = A.qn[id];
-                if (jlo) A.qn[id - sy] = v;
-                if (jhi) A.qn[id + sy] = v;
-                if (klo) {
-                    A.qn[id - 1] = v;
-                    if (jlo) A.qn[id - sy - 1] = v;
-                    if (jhi) A.qn[id + sy - 1] = v;
-                }
-                if (khi) {
-                    A.qn[id + 1] = v;
-                    if (jlo) A.qn[id - sy + 1] = v;
-                    if (jhi) A.qn[id + sy + 1] = v;
-                }
-            }
-        }
-    }
-}
-
-
-// ---------------------------------------------------------------------------
-// ADI line solve along z (the contiguous axis), same arithmetic as
-// k_adi_yz<VAR,2>, but each warp owns 32 neighbouring lines (fixed i,
-// consecutive j) and moves them through shared memory in tiles of 32 lines x
-// ZW positions, so that every global access is a coalesced row segment
-// instead of 32 lines' worth of strided ones.  Forward elimination writes c'
+// ADI line solve along z (the contiguous axis): (1 - fac A) x = S, serial
+// Thomas as tridiag_1rhs (pllcart3d.c:3511-3536; concentration L592-650,
+// xmom L991-1049, ymom L1148-1206, zmom L1300-1354).  Each warp owns 32
+// neighbouring lines (fixed i, consecutive j) and moves them through shared
+// memory in tiles of 32 lines x ZW positions, so that every global access is
+// a coalesced row segment instead of 32 lines' worth of strided ones.  Forward elimination writes c'
 // to `cc` and the eliminated rhs over S, tile by tile; back substitution
 // walks the tiles in reverse.  The recurrence is latency-bound (one
 // dependent chain per lane), so the tiles are kept narrow (ZW = 16) to
@@ -1318,8 +1156,9 @@ __global__ void __launch_bounds__(256) k_adi_y_part(Geo G, Rng R, Consts K, MuPt
 // viscosity value per position) are issued before the dependent Thomas
 // recurrence consumes them, so the sweep streams instead of waiting one
 // memory latency per position.  AXIS 1 is tridiag_1rhs (pllcart3d.c:3511);
-// AXIS 0 is pll_tridiag's one-rank form with the convective outflow, the
-// q_new update and (for c) the Neumann ghosts, as k_adi_x.
+// AXIS 0 is pll_tridiag's one-rank form (pll_tridiag.c:21-47, 96-110) with
+// the convective outflow (e.g. pllcart3d.c:677-683), q_new = q_old + delta
+// and, for c, the Neumann ghosts of pllcart3d.c:700-712.
 // ---------------------------------------------------------------------------
 template <int VAR, int AXIS, typename real>
 __global__ void __launch_bounds__(128) k_line_pf(Geo G, Rng R, Consts K, XsweepArgs<real> A)
