@@ -58,7 +58,11 @@ typedef struct pllgpu_params {
     double Re, Pe, Vratio, Fx, Fy, CFLmax, Timestep, Mum, Lambda;
     int precision;         /* PLLGPU_FP64 or PLLGPU_MIXED                      */
     int exact_dct;         /* 1: DCT sums in sequential order (bitwise with
-                              the CPU restatement); 0: tensor-core DMMA        */
+                              the CPU restatement), and in the precision form
+                              every line / mode solve the sequential Thomas
+                              sweep; 0: tensor-core DCT, and in the precision
+                              form the partitioned line solves and the FP32-
+                              scratch mode solve                              */
     int use_graph;         /* 1: replay each step as one CUDA graph            */
     int dct_kernel;        /* precision form, exact_dct 0: 0 = tcgen05 split-TF32
                               GEMMs (persistent, one CTA per SM) where ny, nz
