@@ -35,7 +35,10 @@ class Solver:
     reductions.  dct_kernel="auto" runs the precision form's DCT passes as
     tcgen05 GEMMs where the plane shape allows (ny, nz in {128, 256}; a
     persistent kernel, one CTA per SM), "umma_tile" the same tcgen05 pass
-    with one tile per CTA, "mma_sync" the warp-level split-TF32 GEMM."""
+    with one tile per CTA, "mma_sync" the warp-level split-TF32 GEMM.
+    exact_dct=True sums the DCTs in sequential order and, in the precision
+    form, runs every line and mode solve as the sequential Thomas sweep (the
+    default runs the partitioned line solves and the paired FP32x2 kernels)."""
 
     def __init__(self, params: Params, device: int = 0, exact_dct: bool = False,
                  use_graph: bool = True, precision: str = "fp64", dct_kernel: str = "auto"):
