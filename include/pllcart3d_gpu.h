@@ -61,8 +61,8 @@ typedef struct pllgpu_params {
                               the CPU restatement), and in the precision form
                               every line / mode solve the sequential Thomas
                               sweep; 0: tensor-core DCT, and in the precision
-                              form the partitioned line solves and the FP32-
-                              scratch mode solve                              */
+                              form the partitioned line solves and, with the
+                              tcgen05 DCT, the FP32-scratch mode solve        */
     int use_graph;         /* 1: replay each step as one CUDA graph            */
     int dct_kernel;        /* precision form, exact_dct 0: 0 = tcgen05 split-TF32
                               GEMMs (persistent, one CTA per SM) where ny, nz

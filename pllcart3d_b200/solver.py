@@ -38,7 +38,8 @@ class Solver:
     with one tile per CTA, "mma_sync" the warp-level split-TF32 GEMM.
     exact_dct=True sums the DCTs in sequential order and, in the precision
     form, runs every line and mode solve as the sequential Thomas sweep (the
-    default: the partitioned line solves and the FP32-scratch mode solve)."""
+    default: the partitioned line solves and, with the tcgen05 DCT, the
+    FP32-scratch mode solve)."""
 
     def __init__(self, params: Params, device: int = 0, exact_dct: bool = False,
                  use_graph: bool = True, precision: str = "fp64", dct_kernel: str = "auto"):
