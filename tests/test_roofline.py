@@ -30,3 +30,28 @@ def test_bytes_scale_with_cells_and_word_size():
     assert roofline.kernel_bytes_per_launch("project", cells, "fp64") == 17 * cells * 8
     assert roofline.kernel_bytes_per_launch("project", cells, "fp32") == 17 * cells * 4
     assert roofline.step_bytes(cells, "fp64") == 2 * roofline.step_bytes(cells, "fp32") == 2424 * cells
+
+
+def test_bench_roofline_picks_the_largest_family():
+    """bench.py's roofline field from a synthetic per-label timing table: the
+    family with the largest total time wins, its achieved bandwidth is its
+    algorithmic bytes over its mean launch time, traffic uses the ncu ratio."""
+    import bench
+
+    cells = 1 << 20
+    kernels = {
+        "explicit_u": {"ms_total": 6.0, "launches": 6},
+        "explicit_v": {"ms_total": 6.0, "launches": 6},
+        "project": {"ms_total": 3.0, "launches": 3},
+        "viscosity": {"ms_total": 1.0, "launches": 3},
+    }
+    r = bench.roofline_of(kernels, 2, cells, "fp32")
+    assert r["kernel"] == "k_explicit2" and r["labels"] == ["explicit_u", "explicit_v"]
+    assert r["bound"] == "hbm" and r["avg_launch_ms"] == 1.0
+    alg = roofline.kernel_bytes_per_launch("explicit_u", cells, "fp32")
+    assert abs(r["achieved"] - alg / 1e-3 / 1e9) < 1e-6
+    assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-12
+    assert abs(r["traffic"] - bench.TRAFFIC_RATIO[("k_explicit2", "fp32")] * alg) < 1.0
+    assert abs(r["share_of_step"] - 12.0 / 16.0) < 1e-12
+    r64 = bench.roofline_of(kernels, 2, cells, "fp64")
+    assert r64["kernel"] == "k_explicit"
