@@ -21,7 +21,7 @@ larger than the 126 MB L2, so no L2 flush is needed between steps.
                   oracle/Makefile, single rank), one process per host core,
                   each timed on a bounded sample of steps of the same
                   workload's physics; cell-steps/s summed over the cores.
-With N>1 (torchrun) every rank advances its own replica (the north-star path
+With N>1 (torchrun) every rank advances its own replica (the timed step path
 runs on one GPU; replicas only) and `value` sums cells over ranks.
 """
 

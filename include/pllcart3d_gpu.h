@@ -197,24 +197,6 @@ int pllgpu_tridiag_batch(int N, int n, const double *a, double *b, double *c,
 int pllgpu_dct2d_batch(int kind, int n0, int n1, int howmany, const double *in,
                        double *out);
 
-/*
- * pllgpu_dct2d_batch without device allocation.  No counterpart in the
- * reference: it exists for callers that cannot allocate device memory
- * themselves or through this library (a host whose pool allocator owns the
- * device's memory; a caller that cannot accept the device synchronisation
- * that cudaMalloc/cudaFree may cause).  d_in and d_out are the caller's
- * device buffers (howmany*n0*n1 doubles each, as pllgpu_dct2d_batch lays
- * them out); the work runs on `stream` (a cudaStream_t, NULL for the legacy
- * default stream) and is not synchronised.  The two cosine matrices and the
- * intermediate array live in one fixed scratch array inside the library of
- * PLLGPU_DCT_NOALLOC_MAX_DOUBLES doubles (16 MiB) per device, held until the
- * process exits: n0*n0 + n1*n1 + howmany*n0*n1 must not exceed it
- * (PLLGPU_EINVAL and a message otherwise).  The first call on a device looks
- * the scratch address up on that device (make it current first).  Calls
- * share the scratch, so calls that overlap on the GPU (other streams, other
- * threads) race; each call overwrites what it reads, so none needs it
- * cleared.
- */
 /* ---- snapshot, restart and diagnostic files ---------------------------- *
  * The reference's output routines on the resident state, writing its file
  * formats into `dir` (NULL: the working directory).  The device packs each
@@ -300,6 +282,28 @@ int pllgpu_copy_state(pllgpu_ctx *dst, pllgpu_ctx *src);
 int pllgpu_pack_cells(pllgpu_ctx *ctx, float *d_cells);
 int pllgpu_unpack_cells(pllgpu_ctx *ctx, const float *d_cells);
 
+/*
+ * pllgpu_dct2d_batch without device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory
+ * themselves or through this library (a host whose pool allocator owns the
+ * device's memory; a caller that cannot accept the device synchronisation
+ * that cudaMalloc/cudaFree may cause).  d_in and d_out are the caller's
+ * device buffers (howmany*n0*n1 doubles each, as pllgpu_dct2d_batch lays
+ * them out); the work runs on `stream` (a cudaStream_t, NULL for the legacy
+ * default stream) and is not synchronised.  The two cosine matrices and the
+ * intermediate array live in one fixed scratch array inside the library of
+ * PLLGPU_DCT_NOALLOC_MAX_DOUBLES doubles (16 MiB) per device, held until the
+ * process exits: n0*n0 + n1*n1 + howmany*n0*n1 must not exceed it
+ * (PLLGPU_EINVAL and a message otherwise, checked without overflow before
+ * any device work).  Any howmany that fits runs (the batch is launched in
+ * chunks of at most 65535 arrays).  The first call on a device looks the
+ * scratch address up on that device (make it current first).  Calls share
+ * the scratch and it keeps the last call's contents, so calls that overlap
+ * on the GPU (other streams, other threads) race; each call overwrites what
+ * it reads, so none needs it cleared.  PLLGPU_ECUDA reports a failed launch
+ * of this call's own kernels; an error left pending by earlier, unrelated
+ * work is neither reported nor cleared.
+ */
 #define PLLGPU_DCT_NOALLOC_MAX_DOUBLES (1L << 21)
 int pllgpu_dct2d_batch_noalloc(int kind, int n0, int n1, int howmany,
                                const double *d_in, double *d_out,

@@ -46,13 +46,14 @@ def oracle_available() -> bool:
     return os.path.exists(ORACLE_LIB)
 
 
-def build(ref: bool = True) -> None:
-    """Build liboracle.so, and the reference library when its sources exist."""
+def build(ref: bool = True, ref_dir: str | None = None) -> None:
+    """Build liboracle.so, and the reference library when its sources exist
+    (in ``ref_dir``, else in the directory PLL_REFERENCE_DIR names)."""
     import subprocess
 
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
-    if ref and os.path.isdir(os.environ.get("PLL_REFERENCE_DIR", "/root/reference")):
-        ref_dir = os.environ.get("PLL_REFERENCE_DIR", "/root/reference")
+    ref_dir = ref_dir or os.environ.get("PLL_REFERENCE_DIR")
+    if ref and ref_dir and os.path.isfile(os.path.join(ref_dir, "pllcart3d.c")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_dir}"], check=True)
 
 

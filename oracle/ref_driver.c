@@ -122,6 +122,26 @@ int pllref_init(const char *rundir)
     return 0;
 }
 
+/* input() (pllcart3d.c:271-350) on <dir>/param.input; its 34 values in
+ * file order, as doubles, into out[34] */
+int pllref_read_input(const char *dir, double *out)
+{
+    char here[4096];
+    int n = 0;
+    if (!getcwd(here, sizeof(here)) || chdir(dir) != 0) return -1;
+    input();
+    if (chdir(here) != 0) return -1;
+    out[n++] = Nx_cell_global; out[n++] = Ny_cell_global; out[n++] = Nz_cell_global;
+    out[n++] = Nx_ghost; out[n++] = Ny_ghost; out[n++] = Nz_ghost;
+    out[n++] = Initial; out[n++] = Ugrid; out[n++] = Niter_print; out[n++] = Out_mid;
+    out[n++] = X1; out[n++] = X2; out[n++] = Y1; out[n++] = Y2; out[n++] = Z1; out[n++] = Z2;
+    out[n++] = Timemax; out[n++] = Timestep; out[n++] = Re; out[n++] = Pe; out[n++] = Vratio;
+    out[n++] = Fx; out[n++] = Fy; out[n++] = Inf_pos; out[n++] = Inf_thick; out[n++] = CFLmax;
+    out[n++] = Out_inter; out[n++] = Wavpert; out[n++] = Ampli; out[n++] = Lamb; out[n++] = Subharm;
+    out[n++] = Nmvp; out[n++] = Mum; out[n++] = Lambda;
+    return n;
+}
+
 void pllref_set_fast_dct(int fast) { pll_shim_fftw_set_fast(fast); }
 
 void pllref_dims(int *d)
@@ -218,6 +238,60 @@ int pllref_get_abc(const char *name, int is, int ie, int js, int je, int ks,
                 b[id] = f[i][j][k].b;
                 c[id] = f[i][j][k].c;
             }
+    return 0;
+}
+
+/* A_conc / A_umom / A_vmom / A_wmom (pllcart3d.c:1411-1536) on the
+ * reference's own structures, from the old (mu_which 0) or new (1)
+ * viscosity, each taken from f[0..3] when given (the drop-in layer's) or
+ * the reference's own.  Before the call the interior of every Tri_abc is
+ * filled with NaN, so a coefficient the called routine does not write shows. */
+typedef void (*ac_fn)(Grid *, Conc *);
+typedef void (*am_fn)(Grid *, Visc *, Velo *);
+
+static void nan_abc(Tri_abc ***f, int is, int ie, int js, int je, int ks, int ke)
+{
+    int i, j, k;
+    for (i = is; i <= ie; i++)
+        for (j = js; j <= je; j++)
+            for (k = ks; k <= ke; k++) f[i][j][k].a = f[i][j][k].b = f[i][j][k].c = NAN;
+}
+
+int pllref_acoef_with(void **f, int mu_which)
+{
+    Visc *mu = mu_which ? g_mu_new : g_mu_old;
+    ac_fn fc = (f && f[0]) ? (ac_fn)f[0] : A_conc;
+    am_fn fu = (f && f[1]) ? (am_fn)f[1] : A_umom;
+    am_fn fv = (f && f[2]) ? (am_fn)f[2] : A_vmom;
+    am_fn fw = (f && f[3]) ? (am_fn)f[3] : A_wmom;
+    nan_abc(g_c->Ax, g_c->istart, g_c->iend, g_c->jstart, g_c->jend, g_c->kstart, g_c->kend);
+    nan_abc(g_c->Ay, g_c->istart, g_c->iend, g_c->jstart, g_c->jend, g_c->kstart, g_c->kend);
+    nan_abc(g_c->Az, g_c->istart, g_c->iend, g_c->jstart, g_c->jend, g_c->kstart, g_c->kend);
+#define NAN3(q) \
+    nan_abc(q->Ax, q->istart, q->iend, q->jstart, q->jend, q->kstart, q->kend); \
+    nan_abc(q->Ay, q->istart, q->iend, q->jstart, q->jend, q->kstart, q->kend); \
+    nan_abc(q->Az, q->istart, q->iend, q->jstart, q->jend, q->kstart, q->kend)
+    NAN3(g_u);
+    NAN3(g_v);
+    NAN3(g_w);
+#undef NAN3
+    fc(g_grid, g_c);
+    fu(g_grid, mu, g_u);
+    fv(g_grid, mu, g_v);
+    fw(g_grid, mu, g_w);
+    return 0;
+}
+
+/* the unknown range of a variable (0 c, 1 u, 2 v, 3 w): is, ie, js, je, ks, ke */
+int pllref_range(int var, int *r)
+{
+    Conc *c = g_c;
+    Velo *q = var == 1 ? g_u : var == 2 ? g_v : g_w;
+    if (var == 0) {
+        r[0] = c->istart; r[1] = c->iend; r[2] = c->jstart; r[3] = c->jend; r[4] = c->kstart; r[5] = c->kend;
+    } else {
+        r[0] = q->istart; r[1] = q->iend; r[2] = q->jstart; r[3] = q->jend; r[4] = q->kstart; r[5] = q->kend;
+    }
     return 0;
 }
 

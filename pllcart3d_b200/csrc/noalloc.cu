@@ -58,18 +58,43 @@ __global__ void k_dct_matrix(int kind, int n, double* T)
 }  // namespace
 }  // namespace pll
 
+namespace pll {
+namespace {
+
+// Scratch doubles a call needs (n0*n0 + n1*n1 + howmany*n0*n1), or -1 when
+// that exceeds the fixed array.  Each term is bounded before it is added,
+// so no product or sum can overflow (n0, n1, howmany >= 1).
+long noalloc_need(int n0, int n1, int howmany)
+{
+    const long cap = (long)PLLGPU_DCT_NOALLOC_MAX_DOUBLES;
+    const long t0 = (long)n0 * n0, t1 = (long)n1 * n1, per = (long)n0 * n1;   // < 2^62 each
+    if (t0 > cap || t1 > cap || per > cap || t0 + t1 > cap) return -1;
+    if ((long)howmany > (cap - t0 - t1) / per) return -1;
+    return t0 + t1 + per * howmany;
+}
+
+// one launch with its own error code (cudaLaunchKernel returns the error of
+// this launch; the thread's pending error is touched only when it failed)
+cudaError_t launch(const void* fn, dim3 grid, dim3 block, void** args, cudaStream_t st)
+{
+    const cudaError_t e = cudaLaunchKernel(fn, grid, block, args, 0, st);
+    if (e != cudaSuccess) (void)cudaGetLastError();   // the error is this launch's; report it by return
+    return e;
+}
+
+}  // namespace
+}  // namespace pll
+
 extern "C" int pllgpu_dct2d_batch_noalloc(int kind, int n0, int n1, int howmany, const double* d_in,
                                           double* d_out, void* stream)
 {
     if ((kind != 0 && kind != 1) || n0 < 1 || n1 < 1 || howmany < 0 || !d_in || !d_out) return PLLGPU_EINVAL;
     if (howmany == 0) return PLLGPU_OK;
-    const long per = (long)n0 * n1;
-    const long need = (long)n0 * n0 + (long)n1 * n1 + per * howmany;
-    if (need > (long)PLLGPU_DCT_NOALLOC_MAX_DOUBLES) {
+    if (noalloc_need(n0, n1, howmany) < 0) {
         std::fprintf(stderr,
-                     "pllgpu_dct2d_batch_noalloc: %d x %d x %d needs %ld doubles of scratch, "
-                     "more than its fixed %ld\n",
-                     howmany, n0, n1, need, (long)PLLGPU_DCT_NOALLOC_MAX_DOUBLES);
+                     "pllgpu_dct2d_batch_noalloc: %d x %d x %d needs more than its fixed scratch of %ld "
+                     "doubles\n",
+                     howmany, n0, n1, (long)PLLGPU_DCT_NOALLOC_MAX_DOUBLES);
         return PLLGPU_EINVAL;
     }
     int dev = 0;
@@ -90,13 +115,38 @@ extern "C" int pllgpu_dct2d_batch_noalloc(int kind, int n0, int n1, int howmany,
     double* T0 = g_scratch_addr[dev];
     double* T1 = T0 + (long)n0 * n0;
     double* tmp = T1 + (long)n1 * n1;
-    k_dct_matrix<<<(int)(((long)n0 * n0 + 255) / 256), 256, 0, st>>>(kind, n0, T0);
-    k_dct_matrix<<<(int)(((long)n1 * n1 + 255) / 256), 256, 0, st>>>(kind, n1, T1);
-    // along the fast dimension, then along the slow one (as pllgpu_dct2d_batch)
-    GemmDesc a{n0, n1, n1, howmany, per, n1, 1, 0, 1, n1, per, n1, 1, 0.0, 0};
-    k_gemm_seq<double><<<dim3((n1 + 63) / 64, (n0 + 63) / 64, howmany), 256, 0, st>>>(a, d_in, T1, tmp);
-    GemmDesc b{n0, n1, n0, howmany, 0, n0, 1, per, n1, 1, per, n1, 1, 0.0, 0};
-    k_gemm_seq<double><<<dim3((n1 + 63) / 64, (n0 + 63) / 64, howmany), 256, 0, st>>>(b, T0, tmp, d_out);
-    if (cudaGetLastError() != cudaSuccess) return PLLGPU_ECUDA;
+    const long per = (long)n0 * n1;
+    {
+        int kd = kind, n = n0;
+        double* T = T0;
+        void* args[] = {&kd, &n, &T};
+        if (launch((const void*)k_dct_matrix, dim3((unsigned)(((long)n0 * n0 + 255) / 256)), dim3(256), args, st) !=
+            cudaSuccess)
+            return PLLGPU_ECUDA;
+        n = n1;
+        T = T1;
+        if (launch((const void*)k_dct_matrix, dim3((unsigned)(((long)n1 * n1 + 255) / 256)), dim3(256), args, st) !=
+            cudaSuccess)
+            return PLLGPU_ECUDA;
+    }
+    // along the fast dimension, then along the slow one (as
+    // pllgpu_dct2d_batch); the batch goes in chunks that fit gridDim.z
+    constexpr int kMaxZ = 65535;
+    for (int b0 = 0; b0 < howmany; b0 += kMaxZ) {
+        const int nb = (howmany - b0) < kMaxZ ? (howmany - b0) : kMaxZ;
+        const double* in = d_in + (long)b0 * per;
+        double* t = tmp + (long)b0 * per;
+        double* out = d_out + (long)b0 * per;
+        const dim3 grid((unsigned)((n1 + 63) / 64), (unsigned)((n0 + 63) / 64), (unsigned)nb);
+        GemmDesc a{n0, n1, n1, nb, per, n1, 1, 0, 1, n1, per, n1, 1, 0.0, 0};
+        const double* B1 = T1;
+        void* args_a[] = {&a, &in, &B1, &t};
+        if (launch((const void*)k_gemm_seq<double>, grid, dim3(256), args_a, st) != cudaSuccess) return PLLGPU_ECUDA;
+        GemmDesc b{n0, n1, n0, nb, 0, n0, 1, per, n1, 1, per, n1, 1, 0.0, 0};
+        const double* A0 = T0;
+        const double* tc = t;
+        void* args_b[] = {&b, &A0, &tc, &out};
+        if (launch((const void*)k_gemm_seq<double>, grid, dim3(256), args_b, st) != cudaSuccess) return PLLGPU_ECUDA;
+    }
     return PLLGPU_OK;
 }

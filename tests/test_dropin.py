@@ -186,3 +186,56 @@ def test_dropin_line_solvers_weno_and_dct():
     assert np.allclose(back, src, rtol=1e-12, atol=1e-12)
     assert L.pllgpu_dropin_status() == 0
     L.pllgpu_finalize()
+
+
+def _abc_all(run, ranges):
+    """Every variable's Ax/Ay/Az triples on its unknown range, from the
+    reference's Tri_abc arrays (NaN elsewhere)."""
+    out = {}
+    lib = run.lib
+    P = ctypes.POINTER(ctypes.c_double)
+    lib.pllref_get_abc.argtypes = [ctypes.c_char_p] + [ctypes.c_int] * 6 + [P] * 3
+    for var, q in enumerate("cuvw"):
+        r = ranges[var]
+        for ax in ("Ax", "Ay", "Az"):
+            a, b, c = (np.full(run.shape, np.nan) for _ in range(3))
+            assert lib.pllref_get_abc(f"{q}_{ax}".encode(), *r, *(pyref._ptr(t) for t in (a, b, c))) == 0
+            sl = tuple(slice(r[2 * d], r[2 * d + 1] + 1) for d in range(3))
+            out[f"{q}_{ax}"] = np.stack([a[sl], b[sl], c[sl]])
+    return out
+
+
+@pytest.mark.parametrize("name,kw", [("fingering-20x8x10", {}), ("fingering-18x9x7", {"Nmvp": 1})])
+def test_dropin_acoef_fills_reference_tri_abc(name, kw):
+    """The drop-in A_conc / A_umom / A_vmom / A_wmom (pllcart3d.c:1411-1536)
+    fill the caller's Tri_abc arrays with the reference's own coefficients:
+    both are called on the same reference structures after two steps, from
+    the old and from the new viscosity; every triple on each variable's
+    unknown range agrees to 1e-14 of the largest coefficient."""
+    wl = workload(name)
+    wl.params = wl.params.replace(**kw)
+    ic = workload_fields(wl)
+    a = pyref.RefRun(wl.params, ic)
+    a.steps(2)
+    L = _dropin(wl.params, a.timestep)
+    fns = ["A_conc", "A_umom", "A_vmom", "A_wmom"]
+    table = (ctypes.c_void_p * 4)(*[ctypes.cast(getattr(L, n), ctypes.c_void_p).value for n in fns])
+    a.lib.pllref_acoef_with.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    a.lib.pllref_range.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    ranges = []
+    for var in range(4):
+        r = (ctypes.c_int * 6)()
+        a.lib.pllref_range(var, r)
+        ranges.append(list(r))
+    for mu_which in (0, 1):
+        assert a.lib.pllref_acoef_with(None, mu_which) == 0
+        want = _abc_all(a, ranges)
+        assert a.lib.pllref_acoef_with(table, mu_which) == 0
+        assert L.pllgpu_dropin_status() == 0
+        got = _abc_all(a, ranges)
+        for key, w in want.items():
+            g = got[key]
+            assert np.isfinite(w).all() and np.isfinite(g).all(), key
+            err = float(np.abs(g - w).max() / np.abs(w).max())
+            assert err <= 1e-14, (key, mu_which, err)
+    L.pllgpu_finalize()

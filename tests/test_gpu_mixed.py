@@ -105,17 +105,6 @@ def test_diagnostics_match_numpy():
     assert d["div_max"] == pytest.approx(np.abs(div).max(), rel=1e-9, abs=1e-12)
 
 
-def test_paired_explicit_one_step():
-    """The precision form's explicit operator computes cells (k, k+32) in
-    pairs with packed FP32x2 instructions; on 64 z cells every thread's
-    second cell is live.  One step agrees with the FP64 step to FP32 level."""
-    wl, a, b = _pair("fingering-64x64x64", 1)
-    assert b.status() == 0
-    for f in ("c_new", "u_new", "v_new", "w_new"):
-        assert rel_maxnorm(b.get(f), a.get(f)) <= 1e-4, f
-    assert rel_maxnorm(b.get("c_new"), a.get("c_new")) <= 1e-6
-
-
 @pytest.mark.parametrize("name", ["fingering-16x128x128", "fingering-8x256x256", "fingering-8x128x256"])
 def test_persistent_tcgen05_dct_equals_per_tile(name):
     """The persistent tcgen05 DCT (one CTA per SM, double-buffered TMEM) runs

@@ -177,3 +177,32 @@ def test_tridiag_and_dct_primitives():
             L.pll_dct2d_exact(kind, n0, n1, T0.ctypes.data_as(P), T1.ctypes.data_as(P),
                               xi.ctypes.data_as(P), out.ctypes.data_as(P), tmp.ctypes.data_as(P))
             assert np.array_equal(g[t], out)
+
+
+@pytest.mark.parametrize("name,steps", [
+    # the 256x128x128 case at its own grid (z tiles over 128 rows, 256-row
+    # x lines, the DCT at K = 128), and one step of the 512x256x256 case
+    # the bench times (256-row z lines, 512-row x lines, K = 256)
+    ("fingering-256x128x128", 3),
+    ("fingering-512x256x256", 1),
+])
+def test_full_steps_match_oracle_at_bench_sizes(name, steps):
+    """The default FP64 step (graph-replayed, the kernels the bench times)
+    against the CPU restatement at the benchmarked grids; every field on its
+    own max-norm at 1e-10."""
+    wl = workload(name)
+    ic = workload_fields(wl)
+    s = _solver(wl.params)
+    s.load_ic(ic)
+    s.step(steps)
+    assert s.status() == 0
+    got = {f: s.get(f) for f in STATE_FIELDS}
+    dt = s.dt
+    s.close()
+    o = OracleRun(wl.params, ic)
+    o.steps(steps)
+    assert dt == pytest.approx(o.dt, rel=1e-12)
+    for f in STATE_FIELDS:
+        e = rel_maxnorm(got[f], o.get(f))
+        assert e <= TOL, f"{f}: rel err {e:.3e} > {TOL}"
+    del o
