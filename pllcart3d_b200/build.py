@@ -1,9 +1,9 @@
 """Build recipe for the in-tree native libraries (sm_100a only).
 
 * ``libpllgpu.so``          - CUDA kernels + runtime + the ``pllgpu_`` C ABI;
-  the FP64 step is compiled with ``--fmad=false`` so that no multiply-add is
-  contracted (the reference's own arithmetic has none), the precision form's
-  FP32 kernels with contraction;
+  the exact FP64 form is compiled with ``--fmad=false`` so that no
+  multiply-add is contracted (the reference's own arithmetic has none), the
+  FP64 form and the precision form's FP32 kernels with contraction;
 * ``libpllnn.so``            - the learned surrogate's BF16 tensor-core kernels
   (convolution forward / backward, pooling, upsampling, Adam);
 * ``libpllcart3d_dropin.so`` - the reference-signature drop-in layer (plain C,
@@ -31,16 +31,16 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xptxas", "-warn-spills"]
 
-# per-source contraction: the FP64 form and everything the drop-in layer and
-# the primitives run reproduce the reference's operation order, so no
-# multiply-add is contracted there; the precision form's FP32 kernels
-# (form_f32.cu) are free to contract.
-CU_SOURCES = {"runtime.cu": "--fmad=false", "form_f64.cu": "--fmad=false",
+# per-source contraction: the exact FP64 form (form_f64x.cu) and everything
+# the drop-in layer's primitives run reproduce the reference's operation
+# order, so no multiply-add is contracted there; the FP64 form (form_f64.cu)
+# and the precision form's FP32 kernels (form_f32.cu) are free to contract.
+CU_SOURCES = {"runtime.cu": "--fmad=false", "form_f64.cu": "--fmad=true", "form_f64x.cu": "--fmad=false",
               "form_f32.cu": "--fmad=true", "primitives.cu": "--fmad=false",
               "noalloc.cu": "--fmad=false", "io.cu": "--fmad=false",
               "wave.cu": "--fmad=false", "ensemble.cu": "--fmad=false"}
 HEADERS = ["common.cuh", "step_kernels.cuh", "aux_kernels.cuh", "dct_kernels.cuh", "host_util.h",
-           "ctx.cuh", "host_common.cuh", "orchestrate.cuh", "forms.h", "umma_dct.cuh"]
+           "ctx.cuh", "host_common.cuh", "orchestrate.cuh", "forms.h", "umma_dct.cuh", "fft_dct.cuh"]
 
 
 def _nvcc() -> str:

@@ -65,6 +65,10 @@ struct pllgpu_ctx {
     double *mode_cc = nullptr, *mode_rr = nullptr;  // FP64 Poisson mode scratch
     double* stage64 = nullptr;  // one padded FP64 field (mixed-form transfers)
     double *lam_y = nullptr, *lam_z = nullptr;
+    // FP64 form's FFT DCT passes (power-of-two planes): per axis (0 y, 1 z)
+    // cos / sin of 2 pi m / N and of pi k / (2N)
+    bool fft_on = false;
+    double2 *fft_tw[2] = {nullptr, nullptr}, *fft_wq[2] = {nullptr, nullptr};
     UmmaPlan um;                // precision form's tensor-core DCT (when shapes allow)
     double* scal = nullptr;     // device scalars (S_*)
     int* status = nullptr;      // device sticky status bits

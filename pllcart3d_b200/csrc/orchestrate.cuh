@@ -12,6 +12,7 @@
 
 #include <type_traits>
 
+#include "fft_dct.cuh"
 #include "forms.h"
 #include "host_common.cuh"
 #include "umma_dct.cuh"
@@ -267,6 +268,56 @@ void launch_poisson_umma(pllgpu_ctx* ctx)
                 UmmaEpi{ny, ctx->G.sx, ctx->G.sy, 1, (float)(p2 ? 1.0 / four_n : four_n), p2 ? 1 : 2, 0}, phi0);
 }
 
+#if !PLL_FP64_EXACT
+// lengths the FFT passes take: powers of two with whole 16-line tiles
+inline bool fft_len_ok(int n) { return n >= 16 && n <= 256 && (n & (n - 1)) == 0; }
+
+template <int N, int KIND, bool CONTIG>
+void fft_launch(pllgpu_ctx* ctx, const FftLines& d, int axis, const double* in, double* out)
+{
+    const unsigned grid = (unsigned)(d.lines / (2 * FFT_PB));
+    k_dct_fft<double, N, KIND, CONTIG><<<grid, FFT_THREADS, fft_smem_bytes<N>(), ctx->st>>>(
+        d, in, out, ctx->fft_tw[axis], ctx->fft_wq[axis]);
+}
+
+template <int KIND, bool CONTIG>
+void fft_pass(pllgpu_ctx* ctx, int N, const FftLines& d, int axis, const double* in, double* out)
+{
+    switch (N) {
+    case 16: fft_launch<16, KIND, CONTIG>(ctx, d, axis, in, out); break;
+    case 32: fft_launch<32, KIND, CONTIG>(ctx, d, axis, in, out); break;
+    case 64: fft_launch<64, KIND, CONTIG>(ctx, d, axis, in, out); break;
+    case 128: fft_launch<128, KIND, CONTIG>(ctx, d, axis, in, out); break;
+    default: fft_launch<256, KIND, CONTIG>(ctx, d, axis, in, out); break;
+    }
+    mark(ctx, "dct_fft");
+}
+
+// the FP64 form's Poisson solve with FFT DCT passes (compact [x][y][z])
+void launch_poisson_fft(pllgpu_ctx* ctx)
+{
+    Bufs<double>& B = ctx->b64;
+    const int nx = ctx->G.nx, ny = ctx->G.ny, nz = ctx->G.nz;
+    const long N = (long)ny * nz;
+    // y lines: (x, z) -> x*N + z, elements step nz; z lines: (x, y) -> x*N + y*nz
+    const FftLines ylines{nx * nz, nz, N, 1, nz, N, 1, nz, 1.0};
+    const FftLines zlines{nx * ny, ny, N, nz, 1, N, nz, 1, 1.0};
+    fft_pass<0, false>(ctx, ny, ylines, 0, B.dct1, B.dct2);
+    fft_pass<0, true>(ctx, nz, zlines, 1, B.dct2, B.dct1);
+    k_poisson_x<double><<<(int)((N + 127) / 128), 128, 0, ctx->st>>>(nx, ny, nz, ctx->K, ctx->lam_y, ctx->lam_z,
+                                                                    B.dct1, ctx->mode_cc, ctx->mode_rr);
+    mark(ctx, "poisson_x");
+    fft_pass<1, false>(ctx, ny, ylines, 0, B.dct1, B.dct2);
+    // into phi's interior, times 1/(4 ny nz) (exact: a power of two)
+    FftLines out = zlines;
+    out.sa_out = ctx->G.sx;
+    out.sb_out = ctx->G.sy;
+    out.scale = 1.0 / (4.0 * (double)N);
+    double* phi0 = B.phi + (long)ctx->Rg.is * ctx->G.sx + (long)ctx->Rg.js * ctx->G.sy + ctx->Rg.ks;
+    fft_pass<1, true>(ctx, nz, out, 1, B.dct2, phi0);
+}
+#endif
+
 // phisolver_dct after its right-hand side is in dct1 (compact [x][y][z])
 template <typename real>
 void launch_poisson(pllgpu_ctx* ctx)
@@ -276,6 +327,13 @@ void launch_poisson(pllgpu_ctx* ctx)
             launch_poisson_umma(ctx);
             return;
         }
+    } else {
+#if !PLL_FP64_EXACT
+        if (ctx->fft_on) {
+            launch_poisson_fft(ctx);
+            return;
+        }
+#endif
     }
     Bufs<real>& B = bufs<real>(ctx);
     const int nx = ctx->G.nx, ny = ctx->G.ny, nz = ctx->G.nz;
@@ -765,6 +823,34 @@ bool setup_umma(pllgpu_ctx* c)
     return true;
 }
 
+#if !PLL_FP64_EXACT
+// twiddle tables of the FFT DCT passes, evaluated in long double and
+// rounded once (arguments reduced exactly: m < N, k < N)
+bool setup_fft(pllgpu_ctx* c)
+{
+    const int len[2] = {c->P.ny, c->P.nz};
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int a = 0; a < 2; ++a) {
+        const int N = len[a];
+        std::vector<double2> tw((size_t)N), wq((size_t)N);
+        for (int m = 0; m < N; ++m) {
+            const long double t = 2.0L * pi * (long double)m / (long double)N;
+            tw[m] = make_double2((double)cosl(t), (double)sinl(t));
+            const long double q = pi * (long double)m / (2.0L * (long double)N);
+            wq[m] = make_double2((double)cosl(q), (double)sinl(q));
+        }
+        c->fft_tw[a] = (double2*)dalloc<double>(c, 2L * N);
+        c->fft_wq[a] = (double2*)dalloc<double>(c, 2L * N);
+        if (!c->fft_tw[a] || !c->fft_wq[a]) return false;
+        if (cudaMemcpy(c->fft_tw[a], tw.data(), sizeof(double2) * N, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(c->fft_wq[a], wq.data(), sizeof(double2) * N, cudaMemcpyHostToDevice) != cudaSuccess)
+            return false;
+    }
+    c->fft_on = true;
+    return true;
+}
+#endif
+
 template <typename real>
 bool alloc_state(pllgpu_ctx* c)
 {
@@ -815,6 +901,10 @@ bool alloc_state(pllgpu_ctx* c)
     if constexpr (std::is_same<real, float>::value) {
         const bool shape_ok = (p->ny == 128 || p->ny == 256) && (p->nz == 128 || p->nz == 256);
         if (shape_ok && !p->exact_dct && p->dct_kernel != 1 && !setup_umma(c)) return false;
+    } else {
+#if !PLL_FP64_EXACT
+        if (!p->exact_dct && fft_len_ok(p->ny) && fft_len_ok(p->nz) && !setup_fft(c)) return false;
+#endif
     }
     return true;
 }

@@ -44,6 +44,7 @@ namespace pll {
 void enqueue_step_any(pllgpu_ctx* ctx)
 {
     if (ctx->mixed) form_enqueue_step_f32(ctx);
+    else if (ctx->P.exact_dct) form_enqueue_step_f64x(ctx);
     else form_enqueue_step_f64(ctx);
 }
 
@@ -119,7 +120,7 @@ namespace pll {
 
 static int materialize_t_any(pllgpu_ctx* ctx)
 {
-    return ctx->mixed ? form_materialize_f32(ctx) : form_materialize_f64(ctx);
+    return ctx->mixed ? form_materialize_f32(ctx) : ctx->P.exact_dct ? form_materialize_f64x(ctx) : form_materialize_f64(ctx);
 }
 
 int materialize(pllgpu_ctx* ctx)
@@ -139,7 +140,7 @@ void* field_ptr(pllgpu_ctx* ctx, int f, bool for_write)
         if (!for_write) f = new_to_old(f);
         else if (materialize(ctx)) return nullptr;
     }
-    return ctx->mixed ? form_field_ptr_f32(ctx, f) : form_field_ptr_f64(ctx, f);
+    return ctx->mixed ? form_field_ptr_f32(ctx, f) : ctx->P.exact_dct ? form_field_ptr_f64x(ctx, f) : form_field_ptr_f64(ctx, f);
 }
 
 }  // namespace pll
@@ -224,7 +225,7 @@ pllgpu_ctx* pllgpu_create(const pllgpu_params* p, int device)
 
     pllgpu_ctx* c = ctx;
     const long ncell = (long)p->nx * p->ny * p->nz;
-    bool ok = ctx->mixed ? form_alloc_f32(c) : form_alloc_f64(c);
+    bool ok = ctx->mixed ? form_alloc_f32(c) : ctx->P.exact_dct ? form_alloc_f64x(c) : form_alloc_f64(c);
     ok = ok && (c->mode_cc = dalloc<double>(c, ncell)) && (c->mode_rr = dalloc<double>(c, ncell)) &&
          (c->lam_y = dalloc<double>(c, p->ny)) && (c->lam_z = dalloc<double>(c, p->nz)) &&
          (c->scal = dalloc<double>(c, S_COUNT)) && (c->work = dalloc<double>(c, 2L * (p->nx + 8))) &&
@@ -352,7 +353,7 @@ int pllgpu_start(pllgpu_ctx* ctx)
     if (!ctx) return PLLGPU_EINVAL;
     CK(cudaSetDevice(ctx->dev));
     if (int e = materialize(ctx)) return e;
-    int e = ctx->mixed ? form_start_f32(ctx) : form_start_f64(ctx);
+    int e = ctx->mixed ? form_start_f32(ctx) : ctx->P.exact_dct ? form_start_f64x(ctx) : form_start_f64(ctx);
     if (e) return e;
     if (int e2 = check_launch(ctx)) return e2;
     CK(cudaStreamSynchronize(ctx->st));
@@ -365,7 +366,7 @@ int pllgpu_resume(pllgpu_ctx* ctx, double tval)
     if (!ctx) return PLLGPU_EINVAL;
     CK(cudaSetDevice(ctx->dev));
     if (int e = materialize(ctx)) return e;
-    int e = ctx->mixed ? form_resume_f32(ctx) : form_resume_f64(ctx);
+    int e = ctx->mixed ? form_resume_f32(ctx) : ctx->P.exact_dct ? form_resume_f64x(ctx) : form_resume_f64(ctx);
     if (e) return e;
     ctx->resync_c = true;
     if (int e2 = check_launch(ctx)) return e2;
@@ -546,7 +547,9 @@ int pllgpu_routine(pllgpu_ctx* ctx, int routine, const double* in, double* out)
     CK(cudaSetDevice(ctx->dev));
     if (routine != PLLGPU_R_SUBSTEP)
         if (int e = materialize(ctx)) return e;
-    int e = ctx->mixed ? form_routine_f32(ctx, routine, in, out) : form_routine_f64(ctx, routine, in, out);
+    int e = ctx->mixed ? form_routine_f32(ctx, routine, in, out)
+            : ctx->P.exact_dct ? form_routine_f64x(ctx, routine, in, out)
+                               : form_routine_f64(ctx, routine, in, out);
     if (e) return e;
     if (int e2 = check_launch(ctx)) return e2;
     CK(cudaStreamSynchronize(ctx->st));
@@ -558,6 +561,7 @@ int pllgpu_diagnostics(pllgpu_ctx* ctx, double* out4)
     if (!ctx || !out4) return PLLGPU_EINVAL;
     CK(cudaSetDevice(ctx->dev));
     if (ctx->mixed) form_diag_f32(ctx);
+    else if (ctx->P.exact_dct) form_diag_f64x(ctx);
     else form_diag_f64(ctx);
     if (int e = check_launch(ctx)) return e;
     CK(cudaMemcpyAsync(out4, ctx->diag + 3L * ni(ctx->Rg), sizeof(double) * 4, cudaMemcpyDeviceToHost, ctx->st));

@@ -11,6 +11,13 @@
 
 #include "common.cuh"
 
+// 1: the exact FP64 form (the reference's divisions, in its order); 0: the
+// FP64 form (WENO5 weights with one division).  Set by the form's
+// translation unit; units that only share the types default to exact.
+#ifndef PLL_FP64_EXACT
+#define PLL_FP64_EXACT 1
+#endif
+
 namespace pll {
 // internal linkage: each translation unit (and so each precision form with
 // its own contraction flags) owns its instantiations
@@ -109,6 +116,45 @@ __device__ __forceinline__ real weno5(real v0, real v1, real v2, real v3, real v
     real at = a1 + a2 + a3;
     return (a1 / at) * c1 + (a2 / at) * c2 + (a3 / at) * c3;
 }
+
+#if !PLL_FP64_EXACT
+// The FP64 form's WENO5: the same nonlinear weights with one division.  The
+// weights a_i = w_i / e_i^2 (e_i = s_i + eps) enter only through the ratio
+// sum(a_i c_i) / sum(a_i), which is unchanged when every a_i is multiplied
+// by (e_1 e_2 e_3)^2 f^6 for any f > 0; that leaves
+// a_1 = w_1 (e_2 e_3 f^2)^2 and so on, with no division.  f = 2^-E, E the
+// exponent of the largest e_i, is exact; since eps >= 1e-6 max(v^2) and every
+// s_i <= 33 max(v^2), every e_i f lies in [1.5e-8, 2), so the products can
+// neither underflow nor overflow.  The result agrees with the six-division
+// sequence to rounding.
+template <>
+__device__ __forceinline__ double weno5<double>(double v0, double v1, double v2, double v3, double v4)
+{
+    const double con1 = 1.0 / 6.0, con2 = 13.0 / 12.0, con3 = 0.25;
+    const double maxd = fmax(fmax(fmax(v0 * v0, v1 * v1), fmax(v2 * v2, v3 * v3)), v4 * v4);
+    const double c1 = con1 * (2.0 * v0 - 7.0 * v1 + 11.0 * v2);
+    const double c2 = con1 * (-v1 + 5.0 * v2 + 2.0 * v3);
+    const double c3 = con1 * (2.0 * v2 + 5.0 * v3 - v4);
+    double t1 = v0 - 2.0 * v1 + v2, t2 = v0 - 4.0 * v1 + 3.0 * v2;
+    const double s1 = con2 * t1 * t1 + con3 * t2 * t2;
+    t1 = v1 - 2.0 * v2 + v3;
+    t2 = v1 - v3;
+    const double s2 = con2 * t1 * t1 + con3 * t2 * t2;
+    t1 = v2 - 2.0 * v3 + v4;
+    t2 = 3.0 * v2 - 4.0 * v3 + v4;
+    const double s3 = con2 * t1 * t1 + con3 * t2 * t2;
+    const double eps = 1.0e-6 * maxd + 1.0e-99;
+    double e1 = s1 + eps, e2 = s2 + eps, e3 = s3 + eps;
+    const long long be = __double_as_longlong(fmax(fmax(e1, e2), e3)) >> 52;   // biased exponent, e > 0
+    const double f = __longlong_as_double((2046LL - be) << 52);                 // 2^-(be - 1023)
+    e1 *= f;
+    e2 *= f;
+    e3 *= f;
+    const double p23 = e2 * e3, p13 = e1 * e3, p12 = e1 * e2;
+    const double a1 = 0.1 * (p23 * p23), a2 = 0.6 * (p13 * p13), a3 = 0.3 * (p12 * p12);
+    return (a1 * c1 + a2 * c2 + a3 * c3) / (a1 + a2 + a3);
+}
+#endif
 
 // The precision form's WENO5: the same weights with four approximate
 // divisions (__fdividef, <= 2 ulp) in place of six IEEE ones.  With the FP32

@@ -205,7 +205,7 @@ def _abc_all(run, ranges):
     return out
 
 
-@pytest.mark.parametrize("name,kw", [("fingering-20x8x10", {}), ("fingering-18x9x7", {"Nmvp": 1})])
+@pytest.mark.parametrize("name,kw", [("fingering-20x8x10", {}), ("fingering-18x9x7", {"Nmvp": 1, "Vratio": 1.0})])
 def test_dropin_acoef_fills_reference_tri_abc(name, kw):
     """The drop-in A_conc / A_umom / A_vmom / A_wmom (pllcart3d.c:1411-1536)
     fill the caller's Tri_abc arrays with the reference's own coefficients:
