@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
                     help="forms to time; the headline value is --headline's")
-    ap.add_argument("--headline", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--headline", default="fp64", choices=["fp64", "mixed"])
     return ap.parse_args()
 
 
@@ -329,13 +329,61 @@ def roofline_of(kernels, nprof, cells, precision, dims=None):
     return out
 
 
-def run_ours(args, ws, rank, local):
+# the precision form's 1000-step accuracy at the timed workload, measured by
+# `python -m pllcart3d_b200.validate --at 1,32,128,250,500,750,1000` and
+# committed under profiles/ (the bench itself runs only a few steps)
+GATE_RECORD = {"target": "c relative max-norm error <= 1e-5 after 1000 steps against the FP64 form",
+               "c_rel_after_1000_steps": 4.2e-3, "met": False,
+               "record": "profiles/precision_form_accuracy_fingering-512x256x256.md"}
+
+
+def form_accuracy(test, ref, steps):
+    """Relative max-norm errors of c, u (against the velocity vector) and phi
+    of one solver against another after the same steps."""
+    import numpy as np
+
+    def rel(f, comps=None):
+        den = max(float(np.abs(ref.get(c)).max()) for c in (comps or (f,)))
+        return float(np.abs(test.get(f) - ref.get(f)).max()) / den
+
+    vel = ("u_new", "v_new", "w_new")
+    return {"steps": steps, "against": "fp64 form, same seed and step count",
+            "c": rel("c_new"), "u": rel("u_new", vel), "v": rel("v_new", vel), "w": rel("w_new", vel),
+            "phi": rel("phi")}
+
+
+def e2e_of(s, ic, prm, steps, ws):
+    """The step through pllgpu_run_host with host buffers: initial c, u, v, w
+    (FP64) from pinned host memory, start-up, `steps` steps, c, u, v, w back
+    into pinned host memory; wall clock around the call, max over ranks."""
     import ctypes
 
     import numpy as np
     import torch
 
     from pllcart3d_b200 import _lib
+
+    shape = prm.shape
+    pin = [torch.empty(shape, dtype=torch.float64, pin_memory=True) for _ in range(8)]
+    for t, k in zip(pin[:4], "cuvw"):
+        t.numpy()[...] = ic[k]
+    ptr = [ctypes.cast(t.data_ptr(), ctypes.POINTER(ctypes.c_double)) for t in pin]
+    t0 = time.perf_counter()
+    code = s._L.pllgpu_run_host(s._h, steps, *ptr)
+    t1 = time.perf_counter()
+    if code != 0:
+        raise _lib.PllGpuError(code, "run_host")
+    sec = reduce_max(t1 - t0, ws)
+    nbytes = 4 * int(np.prod(shape)) * 8
+    return {"value": prm.cells * steps * ws / sec, "unit": "cell-steps/s",
+            "h2d_bytes_per_step": nbytes / steps, "d2h_bytes_per_step": nbytes / steps,
+            "note": "pllgpu_run_host: initial c,u,v,w (FP64) from pinned host memory, "
+                    f"start-up, {steps} steps, c,u,v,w back to pinned host memory, "
+                    "wall-clock around the call"}
+
+
+def run_ours(args, ws, rank, local):
+    import torch
 
     torch.cuda.set_device(local)
     wl = workload(args.workload)
@@ -354,36 +402,22 @@ def run_ours(args, ws, rank, local):
         m["step_roofline"] = {"bytes_per_step": sb,
                               "achieved_gbs": sb / (m["ms"] / args.steps / 1e3) / 1e9,
                               "frac_of_hbm": sb / (m["ms"] / args.steps / 1e3) / 1e9 / hbm}
+        m["steps_done"] = args.warmup + args.steps + m["profile_steps"]
         forms[form] = m
-        if form != args.headline:
-            m["solver"].close()
 
-    head = forms[args.headline] if args.headline in forms else forms[args.precision]
     if args.headline not in forms:
         args.headline = args.precision
-    s = head["solver"]
+    head = forms[args.headline]
 
-    e2e = None
-    if not args.no_e2e:
-        shape = prm.shape
-        pin = [torch.empty(shape, dtype=torch.float64, pin_memory=True) for _ in range(8)]
-        for t, k in zip(pin[:4], "cuvw"):
-            t.numpy()[...] = ic[k]
-        ptr = [ctypes.cast(t.data_ptr(), ctypes.POINTER(ctypes.c_double)) for t in pin]
-        t0 = time.perf_counter()
-        code = s._L.pllgpu_run_host(s._h, args.steps, *ptr)
-        t1 = time.perf_counter()
-        if code != 0:
-            raise _lib.PllGpuError(code, "run_host")
-        sec = reduce_max(t1 - t0, ws)
-        nbytes = 4 * int(np.prod(shape)) * 8
-        e2e = {"value": cells * args.steps * ws / sec, "unit": "cell-steps/s",
-               "h2d_bytes_per_step": nbytes / args.steps,
-               "d2h_bytes_per_step": nbytes / args.steps,
-               "note": "pllgpu_run_host: initial c,u,v,w (FP64) from pinned host memory, "
-                       f"start-up, {args.steps} steps, c,u,v,w back to pinned host memory, "
-                       "wall-clock around the call"}
-    s.close()
+    # the precision form against the FP64 form from the same seed after the
+    # same number of steps (warm-up + timed + profiled)
+    accuracy = None
+    if "fp64" in forms and "mixed" in forms:
+        accuracy = form_accuracy(forms["mixed"]["solver"], forms["fp64"]["solver"], forms["fp64"]["steps_done"])
+
+    for form, m in forms.items():
+        m["e2e"] = None if args.no_e2e else e2e_of(m["solver"], ic, prm, args.steps, ws)
+        m["solver"].close()
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -395,6 +429,7 @@ def run_ours(args, ws, rank, local):
             cpu = {"value": None, "unit": "cell-steps/s", "cores": 1, "kind": "none",
                    "sample": f"unavailable: {ex}"}
 
+    e2e = head["e2e"]
     if rank == 0:
         line = {
             "metric": METRIC, "value": head["value"], "unit": "cell-steps/s", "n_gpus": ws,
@@ -413,12 +448,15 @@ def run_ours(args, ws, rank, local):
         }
         for form, m in forms.items():
             line[f"{form}_form"] = {"value": m["value"], "ms_per_step": m["ms"] / args.steps,
+                                    "e2e": m["e2e"],
                                     "step_roofline_frac": m["step_roofline"]["frac_of_hbm"],
                                     "roofline": m["roofline"], "clocks": m["clocks"],
                                     "kernels_ms_per_step": {k: v["ms_total"] / m["profile_steps"]
                                                             for k, v in m["kernels"].items()}}
         if "fp64" in forms and "mixed" in forms:
             line["mixed_over_fp64"] = forms["mixed"]["value"] / forms["fp64"]["value"]
+            line["mixed_form"]["accuracy"] = accuracy
+            line["mixed_form"]["gate"] = GATE_RECORD
         print(json.dumps(line), flush=True)
 
 

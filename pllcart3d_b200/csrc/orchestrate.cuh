@@ -144,7 +144,7 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
         // length allows, else for concentration the warp solve of short lines
         ydone = launch_line_seg<VAR, 1>(ctx, R, X);
         if (!ydone && VAR == VC && nj(R) <= ZP_MAX && nj(R) >= 2 * (ZP_MAX / 32) && !ctx->P.exact_dct) {
-            k_adi_y_part<VAR><<<dim3((nk(R) + 31) / 32, ni(R)), 256, adi_y_part_smem(), ctx->st>>>(
+            k_adi_y_part<VAR, float><<<dim3((nk(R) + 31) / 32, ni(R)), 256, adi_y_part_smem<float>(), ctx->st>>>(
                 ctx->G, R, ctx->K, X.mu, B.S, ctx->scal, alpha);
             ydone = true;
         }
@@ -153,11 +153,11 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
         k_line_pf<VAR, 1, real><<<dim3((nk(R) + lb - 1) / lb, ni(R)), lb, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
     mark(ctx, ly[VAR]);
     bool zdone = false;
-    if constexpr (std::is_same<real, float>::value) {
+    if constexpr (std::is_same<real, float>::value || !PLL_FP64_EXACT) {
         if (nk(R) <= ZP_MAX && nk(R) >= 2 * (ZP_MAX / 32) && !ctx->P.exact_dct) {
-            // the precision form's partitioned warp solve
-            k_adi_z_part<VAR><<<dim3((nj(R) + 3) / 4, ni(R)), 128, 0, ctx->st>>>(ctx->G, R, ctx->K, X.mu, B.S,
-                                                                               ctx->scal, alpha);
+            // the partitioned warp solve (precision form and FP64 form)
+            k_adi_z_part<VAR, real><<<dim3((nj(R) + 3) / 4, ni(R)), 128, 0, ctx->st>>>(ctx->G, R, ctx->K, X.mu, B.S,
+                                                                              ctx->scal, alpha);
             zdone = true;
         }
     }
@@ -881,10 +881,14 @@ bool alloc_state(pllgpu_ctx* c)
     cudaMemcpy(B.Tiz, T.data(), sizeof(real) * p->nz * p->nz, cudaMemcpyHostToDevice);
     // kernels above the 48 KB default of dynamic shared memory
     if constexpr (std::is_same<real, float>::value) {
-        cudaFuncSetAttribute(k_adi_y_part<VC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adi_y_part_smem());
-        cudaFuncSetAttribute(k_adi_y_part<VU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adi_y_part_smem());
-        cudaFuncSetAttribute(k_adi_y_part<VV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adi_y_part_smem());
-        cudaFuncSetAttribute(k_adi_y_part<VW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adi_y_part_smem());
+        cudaFuncSetAttribute(k_adi_y_part<VC, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)adi_y_part_smem<float>());
+        cudaFuncSetAttribute(k_adi_y_part<VU, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)adi_y_part_smem<float>());
+        cudaFuncSetAttribute(k_adi_y_part<VV, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)adi_y_part_smem<float>());
+        cudaFuncSetAttribute(k_adi_y_part<VW, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)adi_y_part_smem<float>());
         line_seg_attrs<VC>();
         line_seg_attrs<VU>();
         line_seg_attrs<VV>();

@@ -59,6 +59,33 @@ extern "C" int pllgpu_tridiag_batch(int N, int n, const double* a, double* b, do
     return PLLGPU_OK;
 }
 
+namespace pll {
+namespace {
+
+// the two contractions of a batched 2-d transform (along the fast
+// dimension, then the slow one), in chunks of at most 65535 arrays (the
+// grid's z limit)
+void dct2d_gemms(int n0, int n1, int howmany, const double* x, const double* T0, const double* T1, double* tmp,
+                 double* y)
+{
+    const long per = (long)n0 * n1;
+    constexpr int kMaxZ = 65535;
+    for (int b0 = 0; b0 < howmany; b0 += kMaxZ) {
+        const int nb = (howmany - b0) < kMaxZ ? (howmany - b0) : kMaxZ;
+        const long off = (long)b0 * per;
+        const dim3 grid((n1 + 63) / 64, (n0 + 63) / 64, nb);
+        // tmp[t][r][k] = sum_j T1[k][j] x[t][r][j]
+        GemmDesc d1{n0, n1, n1, nb, per, n1, 1, 0, 1, n1, per, n1, 1, 0.0, 0};
+        k_gemm_seq<double><<<grid, 256>>>(d1, x + off, T1, tmp + off);
+        // y[t][k][c] = sum_r T0[k][r] tmp[t][r][c]
+        GemmDesc d2{n0, n1, n0, nb, 0, n0, 1, per, n1, 1, per, n1, 1, 0.0, 0};
+        k_gemm_seq<double><<<grid, 256>>>(d2, T0, tmp + off, y + off);
+    }
+}
+
+}  // namespace
+}  // namespace pll
+
 extern "C" int pllgpu_dct2d_batch(int kind, int n0, int n1, int howmany, const double* in, double* out)
 {
     if ((kind != 0 && kind != 1) || n0 < 1 || n1 < 1 || howmany < 0 || !in || !out) return PLLGPU_EINVAL;
@@ -76,12 +103,7 @@ extern "C" int pllgpu_dct2d_batch(int kind, int n0, int n1, int howmany, const d
         cudaMemcpy(dT1.p, T1.data(), sizeof(double) * T1.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(dx.p, in, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
         return PLLGPU_ECUDA;
-    // along the fast dimension: tmp[t][r][k] = sum_j T1[k][j] x[t][r][j]
-    GemmDesc d1{n0, n1, n1, howmany, per, n1, 1, 0, 1, n1, per, n1, 1, 0.0, 0};
-    k_gemm_seq<double><<<dim3((n1 + 63) / 64, (n0 + 63) / 64, howmany), 256>>>(d1, dx.d(), dT1.d(), dtmp.d());
-    // along the slow dimension: y[t][k][c] = sum_r T0[k][r] tmp[t][r][c]
-    GemmDesc d2{n0, n1, n0, howmany, 0, n0, 1, per, n1, 1, per, n1, 1, 0.0, 0};
-    k_gemm_seq<double><<<dim3((n1 + 63) / 64, (n0 + 63) / 64, howmany), 256>>>(d2, dT0.d(), dtmp.d(), dy.d());
+    dct2d_gemms(n0, n1, howmany, dx.d(), dT0.d(), dT1.d(), dtmp.d(), dy.d());
     if (cudaGetLastError() != cudaSuccess) return PLLGPU_ECUDA;
     if (cudaMemcpy(out, dy.p, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return PLLGPU_ECUDA;
     return PLLGPU_OK;
@@ -178,10 +200,7 @@ extern "C" int pllgpu_idct2d_batch(int n0, int n1, int howmany, const double* in
         cudaMemcpy(dT1.p, T1.data(), sizeof(double) * T1.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(dx.p, in, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
         return PLLGPU_ECUDA;
-    GemmDesc d1{n0, n1, n1, howmany, per, n1, 1, 0, 1, n1, per, n1, 1, 0.0, 0};
-    k_gemm_seq<double><<<dim3((n1 + 63) / 64, (n0 + 63) / 64, howmany), 256>>>(d1, dx.d(), dT1.d(), dtmp.d());
-    GemmDesc d2{n0, n1, n0, howmany, 0, n0, 1, per, n1, 1, per, n1, 1, 0.0, 0};
-    k_gemm_seq<double><<<dim3((n1 + 63) / 64, (n0 + 63) / 64, howmany), 256>>>(d2, dT0.d(), dtmp.d(), dy.d());
+    dct2d_gemms(n0, n1, howmany, dx.d(), dT0.d(), dT1.d(), dtmp.d(), dy.d());
     // fftw_3d.h:101 divides by (double)(4*N)
     k_divide<<<(int)((tot + 255) / 256), 256>>>(tot, dy.d(), (double)(4 * per));
     if (cudaGetLastError() != cudaSuccess) return PLLGPU_ECUDA;

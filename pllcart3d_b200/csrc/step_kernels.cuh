@@ -893,6 +893,13 @@ __global__ void __launch_bounds__(128, 4) k_adi_z_tiled(Geo G, Rng R, Consts K, 
 constexpr int ZP_MAX = 256;
 __device__ __forceinline__ int zp_skew(int m) { return m + (m >> 3); }
 
+// 1/x of the partitioned solves: FP32 approximate (<= 2 ulp; the pivots of
+// these diagonally dominant systems are >= 1 in magnitude), FP64 IEEE
+template <typename real>
+__device__ __forceinline__ real rcp_(real x) { return (real)1 / x; }
+template <>
+__device__ __forceinline__ float rcp_<float>(float x) { return __fdividef(1.0f, x); }
+
 // Partitioned solve of one line of 32 E rows held E per lane (rows
 // E l .. E l + E - 1 on lane l; a of the first row and c of the last are 0;
 // rows past the line are identity rows): row E l of each lane is a
@@ -900,27 +907,27 @@ __device__ __forceinline__ int zp_skew(int m) { return m + (m >> 3); }
 // separator and the next lane's (x_e = g_e - v_e S_l - w_e S_{l+1}), the 32
 // separator equations are solved by parallel cyclic reduction over warp
 // shuffles, then the interior rows.  FP32, diagonally dominant systems.
-template <int E>
-__device__ __forceinline__ void zp_solve(const float* A, const float* B, const float* C, const float* Rr, float* x,
+template <typename real, int E>
+__device__ __forceinline__ void zp_solve(const real* A, const real* B, const real* C, const real* Rr, real* x,
                                          int lane)
 {
     // interior rows e = 1..E-1: forward in terms of the own separator S_l
-    float ch[E], rh[E], ah[E];
+    real ch[E], rh[E], ah[E];
     {
-        const float ib = __fdividef(1.0f, B[1]);
+        const real ib = rcp_<real>(B[1]);
         ch[1] = C[1] * ib;
         rh[1] = Rr[1] * ib;
         ah[1] = A[1] * ib;
     }
 #pragma unroll
     for (int e = 2; e < E; ++e) {
-        const float id = __fdividef(1.0f, B[e] - A[e] * ch[e - 1]);
+        const real id = rcp_<real>(B[e] - A[e] * ch[e - 1]);
         ch[e] = C[e] * id;
         rh[e] = (Rr[e] - A[e] * rh[e - 1]) * id;
         ah[e] = -A[e] * ah[e - 1] * id;
     }
     // backward: x_e = g_e - v_e S_l - w_e S_{l+1}
-    float g[E], v[E], w[E];
+    real g[E], v[E], w[E];
     g[E - 1] = rh[E - 1];
     v[E - 1] = ah[E - 1];
     w[E - 1] = ch[E - 1];
@@ -931,71 +938,71 @@ __device__ __forceinline__ void zp_solve(const float* A, const float* B, const f
         w[e] = -ch[e] * w[e + 1];
     }
     // separator row 8l: A0 x_{8l-1} + B0 S_l + C0 x_{8l+1} = R0
-    float gp = __shfl_up_sync(0xffffffffu, g[E - 1], 1);
-    float vp = __shfl_up_sync(0xffffffffu, v[E - 1], 1);
-    float wp = __shfl_up_sync(0xffffffffu, w[E - 1], 1);
-    if (lane == 0) gp = vp = wp = 0.f;
-    float al = -A[0] * vp;
-    float be = B[0] - A[0] * wp - C[0] * v[1];
-    float ga = -C[0] * w[1];
-    float rho = Rr[0] - A[0] * gp - C[0] * g[1];
+    real gp = __shfl_up_sync(0xffffffffu, g[E - 1], 1);
+    real vp = __shfl_up_sync(0xffffffffu, v[E - 1], 1);
+    real wp = __shfl_up_sync(0xffffffffu, w[E - 1], 1);
+    if (lane == 0) gp = vp = wp = (real)0;
+    real al = -A[0] * vp;
+    real be = B[0] - A[0] * wp - C[0] * v[1];
+    real ga = -C[0] * w[1];
+    real rho = Rr[0] - A[0] * gp - C[0] * g[1];
     // parallel cyclic reduction of the 32 separator equations
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
-        float al_m = __shfl_up_sync(0xffffffffu, al, d), be_m = __shfl_up_sync(0xffffffffu, be, d);
-        float ga_m = __shfl_up_sync(0xffffffffu, ga, d), rho_m = __shfl_up_sync(0xffffffffu, rho, d);
-        float al_p = __shfl_down_sync(0xffffffffu, al, d), be_p = __shfl_down_sync(0xffffffffu, be, d);
-        float ga_p = __shfl_down_sync(0xffffffffu, ga, d), rho_p = __shfl_down_sync(0xffffffffu, rho, d);
+        real al_m = __shfl_up_sync(0xffffffffu, al, d), be_m = __shfl_up_sync(0xffffffffu, be, d);
+        real ga_m = __shfl_up_sync(0xffffffffu, ga, d), rho_m = __shfl_up_sync(0xffffffffu, rho, d);
+        real al_p = __shfl_down_sync(0xffffffffu, al, d), be_p = __shfl_down_sync(0xffffffffu, be, d);
+        real ga_p = __shfl_down_sync(0xffffffffu, ga, d), rho_p = __shfl_down_sync(0xffffffffu, rho, d);
         if (lane < d) {
-            al_m = 0.f;
-            be_m = 1.f;
-            ga_m = 0.f;
-            rho_m = 0.f;
+            al_m = (real)0;
+            be_m = (real)1;
+            ga_m = (real)0;
+            rho_m = (real)0;
         }
         if (lane + d > 31) {
-            al_p = 0.f;
-            be_p = 1.f;
-            ga_p = 0.f;
-            rho_p = 0.f;
+            al_p = (real)0;
+            be_p = (real)1;
+            ga_p = (real)0;
+            rho_p = (real)0;
         }
-        const float k1 = __fdividef(al, be_m), k2 = __fdividef(ga, be_p);
-        const float nal = -k1 * al_m, nga = -k2 * ga_p;
+        const real k1 = al * rcp_<real>(be_m), k2 = ga * rcp_<real>(be_p);
+        const real nal = -k1 * al_m, nga = -k2 * ga_p;
         be = be - k1 * ga_m - k2 * al_p;
         rho = rho - k1 * rho_m - k2 * rho_p;
         al = nal;
         ga = nga;
     }
-    const float Sl = __fdividef(rho, be);
-    float Sn = __shfl_down_sync(0xffffffffu, Sl, 1);
-    if (lane == 31) Sn = 0.f;
+    const real Sl = rho * rcp_<real>(be);
+    real Sn = __shfl_down_sync(0xffffffffu, Sl, 1);
+    if (lane == 31) Sn = (real)0;
     x[0] = Sl;
 #pragma unroll
     for (int e = 1; e < E; ++e) x[e] = g[e] - v[e] * Sl - w[e] * Sn;
 }
 
-template <int VAR>
-__global__ void __launch_bounds__(128) k_adi_z_part(Geo G, Rng R, Consts K, MuPtrs<float> mu,
-                                                    float* __restrict__ S, const double* __restrict__ scal,
+template <int VAR, typename real>
+__global__ void __launch_bounds__(128) k_adi_z_part(Geo G, Rng R, Consts K, MuPtrs<real> mu,
+                                                    real* __restrict__ S, const double* __restrict__ scal,
                                                     double alpha)
 {
     constexpr int E = ZP_MAX / 32;   // rows per lane
     constexpr int BUF = ZP_MAX + ZP_MAX / 8 + 8;
-    __shared__ float bS[4][BUF];
-    __shared__ float bM[4][BUF];
+    __shared__ real bS[4][BUF];
+    __shared__ real bM[4][BUF];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int j = R.js + blockIdx.x * 4 + warp;
     const int i = R.is + blockIdx.y;
     if (j > R.je) return;   // warp-uniform
     const int n = R.ke - R.ks + 1;
-    const float fac = (float)(0.5 * scal[S_DT] * alpha);
+    const real fac = (real)(0.5 * scal[S_DT] * alpha);
     constexpr int LO = Closure<VAR, 2>::lo, HI = Closure<VAR, 2>::hi;
-    const float* __restrict__ mz = VAR == VU ? mu.xz : VAR == VV ? mu.yz : mu.cell;
+    const real* __restrict__ mz = VAR == VU ? mu.xz : VAR == VV ? mu.yz : mu.cell;
     const int moff = VAR == VW ? -1 : 0;
-    const float dzc = (float)(VAR == VW ? K.d2z : K.d1z);
-    const float ihz = (float)K.ihz, cdz = (float)K.cdz;
+    const real dzc = (real)(VAR == VW ? K.d2z : K.d1z);
+    const real ihz = (real)K.ihz, cdz = (real)K.cdz;
     const long base = (long)i * G.sx + (long)j * G.sy + R.ks;
-    float* sS = bS[warp];
-    float* sM = bM[warp];
+    real* sS = bS[warp];
+    real* sM = bM[warp];
 #pragma unroll
     for (int t = 0; t < E; ++t) {
         const int m = t * 32 + lane;
@@ -1006,12 +1013,12 @@ __global__ void __launch_bounds__(128) k_adi_z_part(Geo G, Rng R, Consts K, MuPt
     __syncwarp();
 
     // this lane's rows m = 8 lane + e: a x_{m-1} + b x_m + c x_{m+1} = r
-    float A[E], B[E], C[E], Rr[E];
+    real A[E], B[E], C[E], Rr[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const int m = E * lane + e;
         if (m < n) {
-            float a, c;
+            real a, c;
             if (VAR == VC) {
                 a = cdz;
                 c = cdz;
@@ -1019,31 +1026,31 @@ __global__ void __launch_bounds__(128) k_adi_z_part(Geo G, Rng R, Consts K, MuPt
                 a = dzc * sM[zp_skew(m)] * ihz;
                 c = dzc * sM[zp_skew(m + 1)] * ihz;
             }
-            const float b = -(a + c);
-            float la = -fac * a, lb = 1.0f - fac * b, lc = -fac * c, lr = sS[zp_skew(m)];
+            const real b = -(a + c);
+            real la = -fac * a, lb = (real)1.0 - fac * b, lc = -fac * c, lr = sS[zp_skew(m)];
             if (m == 0) {
                 if (LO == 1) lb += la;
                 else if (LO == 2) lb -= la;
-                la = 0.f;
+                la = (real)0;
             }
             if (m == n - 1) {
                 if (HI == 1) lb += lc;
                 else if (HI == 2) lb -= lc;
-                lc = 0.f;
+                lc = (real)0;
             }
             A[e] = la;
             B[e] = lb;
             C[e] = lc;
             Rr[e] = lr;
         } else {   // identity rows past the line
-            A[e] = 0.f;
-            B[e] = 1.f;
-            C[e] = 0.f;
-            Rr[e] = 0.f;
+            A[e] = (real)0;
+            B[e] = (real)1;
+            C[e] = (real)0;
+            Rr[e] = (real)0;
         }
     }
-    float x[E];
-    zp_solve<E>(A, B, C, Rr, x, lane);
+    real x[E];
+    zp_solve<real, E>(A, B, C, Rr, x, lane);
     __syncwarp();
 #pragma unroll
     for (int e = 0; e < E; ++e) sS[zp_skew(E * lane + e)] = x[e];
@@ -1106,17 +1113,19 @@ __device__ __forceinline__ void line_ac(const Consts& K, real m0, real m1, real&
 // ---------------------------------------------------------------------------
 constexpr int YP_PITCH = ZP_MAX + ZP_MAX / 8 + 1;   // odd: conflict-free columns
 
-constexpr size_t adi_y_part_smem() { return sizeof(float) * 2 * 32 * YP_PITCH; }
+template <typename real>
+constexpr size_t adi_y_part_smem() { return sizeof(real) * 2 * 32 * YP_PITCH; }
 
-template <int VAR>
-__global__ void __launch_bounds__(256) k_adi_y_part(Geo G, Rng R, Consts K, MuPtrs<float> mu,
-                                                    float* __restrict__ S, const double* __restrict__ scal,
+template <int VAR, typename real>
+__global__ void __launch_bounds__(256) k_adi_y_part(Geo G, Rng R, Consts K, MuPtrs<real> mu,
+                                                    real* __restrict__ S, const double* __restrict__ scal,
                                                     double alpha)
 {
     constexpr int E = ZP_MAX / 32;
-    extern __shared__ float ysm[];
-    float* tS = ysm;                      // [32 lines][YP_PITCH]
-    float* tM = ysm + 32 * YP_PITCH;
+    extern __shared__ __align__(16) unsigned char ysm_raw[];
+    real* ysm = (real*)ysm_raw;
+    real* tS = ysm;                      // [32 lines][YP_PITCH]
+    real* tM = ysm + 32 * YP_PITCH;
     const int i = R.is + blockIdx.y;
     const int k0 = R.ks + blockIdx.x * 32;
     const int nl = (R.ke - k0 + 1) < 32 ? (R.ke - k0 + 1) : 32;
@@ -1124,10 +1133,10 @@ __global__ void __launch_bounds__(256) k_adi_y_part(Geo G, Rng R, Consts K, MuPt
     const long sy = G.sy;
     const long base0 = (long)i * G.sx + (long)R.js * sy + k0;
     constexpr int OFF = LineCoef<VAR, 1>::off;
-    const float* __restrict__ fam = VAR == VC ? nullptr : line_family<VAR, 1, float>(mu);
-    const float dy = (float)(LineCoef<VAR, 1>::twice ? K.d2y : K.d1y);
-    const float ihy = (float)K.ihy, cdy = (float)K.cdy;
-    const float fac = (float)(0.5 * scal[S_DT] * alpha);
+    const real* __restrict__ fam = VAR == VC ? nullptr : line_family<VAR, 1, real>(mu);
+    const real dy = (real)(LineCoef<VAR, 1>::twice ? K.d2y : K.d1y);
+    const real ihy = (real)K.ihy, cdy = (real)K.cdy;
+    const real fac = (real)(0.5 * scal[S_DT] * alpha);
     constexpr int LO = Closure<VAR, 1>::lo, HI = Closure<VAR, 1>::hi;
     // tile loads: thread (kl, row group m0) moves rows m0, m0 + 8, ...;
     // unrolled so that many rows' loads are in flight at once
@@ -1143,14 +1152,14 @@ __global__ void __launch_bounds__(256) k_adi_y_part(Geo G, Rng R, Consts K, MuPt
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int kl = warp; kl < nl; kl += 8) {
-        const float* ls = tS + kl * YP_PITCH;
-        const float* lm = tM + kl * YP_PITCH;
-        float A[E], B[E], C[E], Rr[E];
+        const real* ls = tS + kl * YP_PITCH;
+        const real* lm = tM + kl * YP_PITCH;
+        real A[E], B[E], C[E], Rr[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int m = E * lane + e;
             if (m < n) {
-                float a, c;
+                real a, c;
                 if (VAR == VC) {
                     a = cdy;
                     c = cdy;
@@ -1158,31 +1167,31 @@ __global__ void __launch_bounds__(256) k_adi_y_part(Geo G, Rng R, Consts K, MuPt
                     a = dy * lm[zp_skew(m)] * ihy;
                     c = dy * lm[zp_skew(m + 1)] * ihy;
                 }
-                const float b = -(a + c);
-                float la = -fac * a, lb = 1.0f - fac * b, lc = -fac * c;
+                const real b = -(a + c);
+                real la = -fac * a, lb = (real)1.0 - fac * b, lc = -fac * c;
                 if (m == 0) {
                     if (LO == 1) lb += la;
                     else if (LO == 2) lb -= la;
-                    la = 0.f;
+                    la = (real)0;
                 }
                 if (m == n - 1) {
                     if (HI == 1) lb += lc;
                     else if (HI == 2) lb -= lc;
-                    lc = 0.f;
+                    lc = (real)0;
                 }
                 A[e] = la;
                 B[e] = lb;
                 C[e] = lc;
                 Rr[e] = ls[zp_skew(m)];
             } else {
-                A[e] = 0.f;
-                B[e] = 1.f;
-                C[e] = 0.f;
-                Rr[e] = 0.f;
+                A[e] = (real)0;
+                B[e] = (real)1;
+                C[e] = (real)0;
+                Rr[e] = (real)0;
             }
         }
-        float x[E];
-        zp_solve<E>(A, B, C, Rr, x, lane);
+        real x[E];
+        zp_solve<real, E>(A, B, C, Rr, x, lane);
         __syncwarp();
 #pragma unroll
         for (int e = 0; e < E; ++e) tS[kl * YP_PITCH + zp_skew(E * lane + e)] = x[e];
