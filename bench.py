@@ -17,10 +17,12 @@ larger than the 126 MB L2, so no L2 flush is needed between steps.
                   solver's stream, max over ranks; `e2e` goes through
                   pllgpu_run_host with pinned host buffers (initial fields
                   in, c/u/v/w out, inside the timed region).
---impl reference  the reference's own CPU step (pllcart3d.c compiled by
-                  oracle/Makefile, single rank), one process per host core,
-                  each timed on a bounded sample of steps of the same
-                  workload's physics; cell-steps/s summed over the cores.
+--impl reference  the reference's own CPU step (pllcart3d.c and
+                  pll_tridiag.c compiled by oracle/Makefile) at the same
+                  workload and grid, on its x-slab MPI decomposition over
+                  every host core the slabs allow (processes over a
+                  shared-memory MPI stand-in); a time budget caps the timed
+                  steps.
 With N>1 (torchrun) every rank advances its own replica (the timed step path
 runs on one GPU; replicas only) and `value` sums cells over ranks.
 """
@@ -160,73 +162,65 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_sample(wl_name, seconds=12.0):
-    """The reference CPU step (oracle/_ref, else the CPU restatement) on a
-    bounded sample: a 64x32x32 grid of the workload's physics, stepped until
-    ~`seconds` of single-core work; returns (cell-steps/s, kind, sample)."""
-    from oracle.pyref import OracleRun, RefRun, ref_available
+def ref_ranks(nx):
+    """Ranks of the reference's slab decomposition on this host: every core,
+    as far as the slabs allow (each needs the 3 planes its neighbours'
+    halos read)."""
+    return max(1, min(os.cpu_count() or 1, nx // 3))
 
+
+def ref_mpi(wl_name, ranks, warm, steps, budget_s):
+    """The reference's own multi-rank step (pllcart3d.c on its x-slab
+    decomposition, pll_tridiag.c's pipelined x solves, the halo exchanges)
+    over the shared-memory MPI stand-in, in a fresh process (it forks its
+    ranks, which a process holding a CUDA context must not do)."""
+    cmd = [sys.executable, "-m", "oracle.refmpi", "--workload", wl_name, "--ranks", str(ranks),
+           "--warmup", str(warm), "--steps", str(steps), "--budget", str(budget_s)]
+    out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=1800)
+    if out.returncode != 0:
+        raise RuntimeError(out.stderr.strip().splitlines()[-1] if out.stderr.strip() else "reference run failed")
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def cpu_sample(wl_name, seconds=20.0):
+    """The CPU baseline: the reference's own step at the workload's grid on
+    every host core its slab decomposition allows, one untimed step then
+    timed steps for about `seconds`; returns (cell-steps/s, kind, sample,
+    cores)."""
     wl = workload(wl_name)
-    small = wl.params.replace(Nx_cell_global=64, Ny_cell_global=32, Nz_cell_global=32)
-    ic = workload_fields(type(wl)(wl.name, small, wl.modes, wl.amplitude, wl.steps, wl.seed))
-    if ref_available():
-        run, kind = RefRun(small, ic), "reference"
-        run.set_fast_dct(True)
-    else:
-        run, kind = OracleRun(small, ic), "port"
-        run.set_fast_dct(True)
-    run.steps(1)
-    t0 = time.perf_counter()
-    n = 0
-    while time.perf_counter() - t0 < seconds:
-        run.steps(1)
-        n += 1
-    dt = time.perf_counter() - t0
-    cells = small.cells
-    sample = (f"{n} steps of a 64x32x32 grid with the {wl.name} physics, "
-              f"single core, FFT-based DCT stand-in for FFTW")
-    return cells * n / dt, kind, sample, n
-
-
-def _ref_worker(wl_name, seconds, q):
-    v, kind, sample, n = cpu_sample(wl_name, seconds=seconds)
-    q.put((v, kind, sample))
+    ranks = ref_ranks(wl.params.nx)
+    r = ref_mpi(wl_name, ranks, 1, 1000, seconds)
+    sample = (f"{r['steps']} step(s) of {wl.name} ({wl.params.nx}x{wl.params.ny}x{wl.params.nz}) after 1 untimed "
+              f"step: the reference's pllcart3d.c on {ranks} x-slab ranks (processes over a shared-memory MPI "
+              f"stand-in), FFT-based DCT stand-in for FFTW, {r['seconds']:.1f} s timed")
+    return r["cell_steps_per_s"], "reference", sample, ranks
 
 
 def run_reference(args, ws, rank):
-    """The reference's own CPU step on every host core: one single-rank
-    reference process per core (independent replicas, no communication, so
-    an upper bound on what its MPI decomposition reaches on these cores),
-    each a bounded sample of the workload; cell-steps/s summed over cores."""
+    """The reference's own CPU step on the host cores: pllcart3d.c on its
+    x-slab decomposition over every core the slabs allow (the MPI path of
+    pllcart3d.c:357-378 and pll_tridiag.c), at the benchmarked workload's
+    grid; one untimed step, then up to --steps timed steps within a time
+    budget so that the run ends within minutes."""
     if rank != 0:
         return
-    import multiprocessing as mp
-
     wl = workload(args.workload)
-    cores = os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
-    vals, kind, sample = [], "reference", ""
-    for s in range(args.warmup + args.steps):
-        q = ctx.Queue()
-        procs = [ctx.Process(target=_ref_worker, args=(args.workload, 2.0, q)) for _ in range(cores)]
-        for p in procs:
-            p.start()
-        res = [q.get(timeout=600) for _ in procs]
-        for p in procs:
-            p.join(timeout=60)
-        kind, sample = res[0][1], res[0][2]
-        if s >= args.warmup:
-            vals.append(sum(r[0] for r in res))
-    value = statistics.mean(vals)
+    ranks = ref_ranks(wl.params.nx)
+    budget = 150.0
+    r = ref_mpi(args.workload, ranks, 1, args.steps, budget)
+    value = r["cell_steps_per_s"]
+    sample = (f"{r['steps']} of {args.steps} requested step(s) of {wl.name} after 1 untimed step (a {budget:.0f} s "
+              f"budget caps the timed steps): pllcart3d.c on {ranks} x-slab ranks over a shared-memory MPI "
+              f"stand-in, FFT-based DCT stand-in for FFTW")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-steps/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": args.gpus, "steps": r["steps"], "warmup": 1, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": wl.name, "grid": [wl.params.nx, wl.params.ny, wl.params.nz],
-                   "precision": "fp64"},
-        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": cores, "kind": kind,
-                         "sample": f"{cores} processes, each: " + sample + " per step"},
+                   "precision": "fp64", "parallelism": f"mpi{ranks} (x slabs, host cores)"},
+        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": ranks, "kind": "reference",
+                         "sample": sample},
         "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -422,11 +416,10 @@ def run_ours(args, ws, rank, local):
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
-            v, kind, sample, n = cpu_sample(args.workload, seconds=12.0)
-            cpu = {"value": v, "unit": "cell-steps/s", "cores": 1, "kind": kind,
-                   "sample": sample}
+            v, kind, sample, cores = cpu_sample(args.workload, seconds=20.0)
+            cpu = {"value": v, "unit": "cell-steps/s", "cores": cores, "kind": kind, "sample": sample}
         except Exception as ex:  # the checker may be absent on a bare box
-            cpu = {"value": None, "unit": "cell-steps/s", "cores": 1, "kind": "none",
+            cpu = {"value": None, "unit": "cell-steps/s", "cores": 0, "kind": "none",
                    "sample": f"unavailable: {ex}"}
 
     e2e = head["e2e"]

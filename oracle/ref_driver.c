@@ -95,14 +95,16 @@ static double ***g_phi, ***g_div;
 static double g_tval, g_dt, g_cm;
 static char g_rundir[4096]; /* where the reference's side files go */
 
-int pllref_init(const char *rundir)
+/* set-up of rank `rank` of `size` (pllcart3d.c:57-80 up to the initial
+ * condition); pllref_init is the single-rank case */
+int pllref_init_ranked(const char *rundir, int rank, int size)
 {
     char here[4096];
     if (!getcwd(here, sizeof(here))) return -1;
     if (chdir(rundir) != 0) return -1;
     strncpy(g_rundir, rundir, sizeof(g_rundir) - 1);
-    Rank = 0;
-    Size = 1;
+    Rank = rank;
+    Size = size;
     input();
     g_grid = (Grid *)malloc(sizeof(Grid));
     grid_setup(g_grid);
@@ -121,6 +123,11 @@ int pllref_init(const char *rundir)
     if (chdir(here) != 0) return -1;
     return 0;
 }
+
+int pllref_init(const char *rundir) { return pllref_init_ranked(rundir, 0, 1); }
+
+/* first global x cell of this rank's slab (grid_setup, pllcart3d.c:376-379) */
+int pllref_x_offset(void) { return g_grid->nx_global_offset; }
 
 /* input() (pllcart3d.c:271-350) on <dir>/param.input; its 34 values in
  * file order, as doubles, into out[34] */

@@ -68,6 +68,7 @@ struct pllgpu_ctx {
     // FP64 form's FFT DCT passes (power-of-two planes): per axis (0 y, 1 z)
     // cos / sin of 2 pi m / N and of pi k / (2N)
     bool fft_on = false;
+    bool xt_on = false;         // FP64 form: TMA-staged marching explicit operator
     double2 *fft_tw[2] = {nullptr, nullptr}, *fft_wq[2] = {nullptr, nullptr};
     UmmaPlan um;                // precision form's tensor-core DCT (when shapes allow)
     double* scal = nullptr;     // device scalars (S_*)

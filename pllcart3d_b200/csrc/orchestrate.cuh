@@ -12,6 +12,7 @@
 
 #include <type_traits>
 
+#include "explicit_tma.cuh"
 #include "fft_dct.cuh"
 #include "forms.h"
 #include "host_common.cuh"
@@ -25,6 +26,56 @@ const double kRK1[3] = {(8.0 / 15.0), (5.0 / 12.0), (3.0 / 4.0)};
 const double kRK2[3] = {(0.0), (-17.0 / 60.0), (-5.0 / 12.0)};
 
 // ---- stage launchers --------------------------------------------------------
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled();
+
+// 3-d tensor map of one padded field ([i][j][k], k contiguous, row pitch sy,
+// plane pitch sx) with boxes of box_k x box_j x 1 elements; zeros outside
+template <typename real>
+bool field_map(CUtensorMap* m, const real* base, const Geo& G, int box_k, int box_j)
+{
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn || ((uintptr_t)base & 15) || (G.sy * (long)sizeof(real)) % 16 || (box_k * (int)sizeof(real)) % 16)
+        return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)G.NZ, (cuuint64_t)G.NY, (cuuint64_t)G.NX};
+    const cuuint64_t strides[2] = {(cuuint64_t)(G.sy * (long)sizeof(real)), (cuuint64_t)(G.sx * (long)sizeof(real))};
+    const cuuint32_t box[3] = {(cuuint32_t)box_k, (cuuint32_t)box_j, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return fn(m, sizeof(real) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)base,
+              dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// the TMA-staged plane-marching explicit operator (explicit_tma.cuh); false
+// when a tensor map cannot be made (the caller then runs k_explicit)
+template <typename real, int VAR>
+bool launch_explicit_tma(pllgpu_ctx* ctx, const ExplicitArgs<real>& A)
+{
+    using GM = XtGeom<real>;
+    const Rng& R = ctx->Rv[VAR];
+    XtMaps M;
+    std::memset(&M, 0, sizeof(M));
+    const real* staged[5] = {};
+    if (VAR == VC) {
+        staged[0] = A.vn; staged[1] = A.wn;
+    } else if (VAR == VU) {
+        staged[0] = A.vn; staged[1] = A.wn; staged[2] = A.mu.xy; staged[3] = A.mu.xz;
+    } else if (VAR == VV) {
+        staged[0] = A.un; staged[1] = A.wn; staged[2] = A.mu.yz; staged[3] = A.mu.cell; staged[4] = A.cn;
+    } else {
+        staged[0] = A.un; staged[1] = A.vn; staged[2] = A.mu.yz; staged[3] = A.mu.cell;
+    }
+    if (!field_map<real>(&M.q, A.q, ctx->G, GM::KB3, GM::JB3)) return false;
+    for (int a = 0; a < XtSet<VAR>::NA; ++a)
+        if (!field_map<real>(&M.a[a], staged[a], ctx->G, GM::KB1, GM::JB1)) return false;
+    const dim3 grid((ctx->G.nz + XT_TK - 1) / XT_TK, (nj(R) + XT_TJ - 1) / XT_TJ, (ni(R) + XT_NI - 1) / XT_NI);
+    k_explicit_tma<VAR, real><<<grid, XT_THREADS, XtSmem<real, VAR>::DYN, ctx->st>>>(M, ctx->G, R, ctx->K, A,
+                                                                                     ctx->status);
+    return true;
+}
 
 template <typename real, int VAR>
 void launch_explicit(pllgpu_ctx* ctx, const real* un, const real* vn, const real* wn, double g, double r)
@@ -55,8 +106,10 @@ void launch_explicit(pllgpu_ctx* ctx, const real* un, const real* vn, const real
         const dim3 grid((nk(R) + 2 * EP_DK - 1) / (2 * EP_DK), (nj(R) + blk.y - 1) / blk.y, ni(R));
         k_explicit2<VAR><<<grid, blk, 0, ctx->st>>>(ctx->G, R, ctx->K, A);
     } else {
-        const dim3 blk(bx, by);
-        k_explicit<VAR, real><<<box_grid(nk(R), nj(R), ni(R), blk), blk, 0, ctx->st>>>(ctx->G, R, ctx->K, A);
+        if (!ctx->xt_on || !launch_explicit_tma<real, VAR>(ctx, A)) {
+            const dim3 blk(bx, by);
+            k_explicit<VAR, real><<<box_grid(nk(R), nj(R), ni(R), blk), blk, 0, ctx->st>>>(ctx->G, R, ctx->K, A);
+        }
     }
     mark(ctx, lab[VAR]);
 }
@@ -752,9 +805,6 @@ float tf32_rna_host(float x)
     return r;
 }
 
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 EncodeTiledFn encode_tiled()
 {
@@ -908,6 +958,17 @@ bool alloc_state(pllgpu_ctx* c)
     } else {
 #if !PLL_FP64_EXACT
         if (!p->exact_dct && fft_len_ok(p->ny) && fft_len_ok(p->nz) && !setup_fft(c)) return false;
+        if (!p->exact_dct && c->nelem < (1L << 31) && encode_tiled()) {
+            cudaFuncSetAttribute(k_explicit_tma<VC, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 XtSmem<double, VC>::DYN);
+            cudaFuncSetAttribute(k_explicit_tma<VU, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 XtSmem<double, VU>::DYN);
+            cudaFuncSetAttribute(k_explicit_tma<VV, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 XtSmem<double, VV>::DYN);
+            cudaFuncSetAttribute(k_explicit_tma<VW, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 XtSmem<double, VW>::DYN);
+            c->xt_on = true;
+        }
 #endif
     }
     return true;
