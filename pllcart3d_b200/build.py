@@ -40,7 +40,7 @@ CU_SOURCES = {"runtime.cu": "--fmad=false", "form_f64.cu": "--fmad=true", "form_
               "noalloc.cu": "--fmad=false", "io.cu": "--fmad=false",
               "wave.cu": "--fmad=false", "ensemble.cu": "--fmad=false"}
 HEADERS = ["common.cuh", "step_kernels.cuh", "aux_kernels.cuh", "dct_kernels.cuh", "host_util.h",
-           "ctx.cuh", "host_common.cuh", "orchestrate.cuh", "forms.h", "umma_dct.cuh", "fft_dct.cuh"]
+           "ctx.cuh", "host_common.cuh", "orchestrate.cuh", "forms.h", "umma_dct.cuh", "fft_dct.cuh", "explicit_tma.cuh"]
 
 
 def _nvcc() -> str:

@@ -262,12 +262,6 @@ __global__ void __launch_bounds__(XT_THREADS) k_explicit_tma(const __grid_consta
             };
             auto QT = [&](int dj, int dk) -> real { return Q[o3 + dj * KB3 + dk]; };
             const real hf = (real)0.5, qr = (real)0.25;
-            real vy[7], vz[7];
-#pragma unroll
-            for (int t = 0; t < 7; ++t) {
-                vy[t] = QT(t - 3, 0);
-                vz[t] = QT(0, t - 3);
-            }
             // advecting velocities (adv_vel)
             real ux, uy, uz;
             if (VAR == VC) {
@@ -287,9 +281,25 @@ __global__ void __launch_bounds__(XT_THREADS) k_explicit_tma(const __grid_consta
                 uy = qr * (T(1, 0, 0, -1) + T(1, 0, 0, 0) + T(1, 0, 1, -1) + T(1, 0, 1, 0));
                 uz = qx[3];
             }
+            // one stencil window at a time (y, then z) keeps register use low
             const real cx = ux * xt_upwind<0, real>(qx, q, G, R, K, i, ux);
-            const real cy = uy * xt_upwind<1, real>(vy, q, G, R, K, j, uy);
-            const real cz = uz * xt_upwind<2, real>(vz, q, G, R, K, k, uz);
+            real cy, cz, qym, qyp, qzm, qzp;
+            {
+                real vy[7];
+#pragma unroll
+                for (int t = 0; t < 7; ++t) vy[t] = QT(t - 3, 0);
+                cy = uy * xt_upwind<1, real>(vy, q, G, R, K, j, uy);
+                qym = vy[2];
+                qyp = vy[4];
+            }
+            {
+                real vz[7];
+#pragma unroll
+                for (int t = 0; t < 7; ++t) vz[t] = QT(0, t - 3);
+                cz = uz * xt_upwind<2, real>(vz, q, G, R, K, k, uz);
+                qzm = vz[2];
+                qzp = vz[4];
+            }
             const real ct = cz + cx + cy;
             real H;
             if (VAR == VC) {
@@ -343,7 +353,7 @@ __global__ void __launch_bounds__(XT_THREADS) k_explicit_tma(const __grid_consta
                 c = over_h<real>((real)K.d1y * T(2, 0, 1, 0), K.hy, K.ihy, K.pow2);
             }
             b = -(a + c);
-            const real ay = a * vy[2] + b * vy[3] + c * vy[4];
+            const real ay = a * qym + b * qx[3] + c * qyp;
             if (VAR == VC) {
                 a = c = (real)K.cdz;
             } else if (VAR == VU) {
@@ -357,7 +367,7 @@ __global__ void __launch_bounds__(XT_THREADS) k_explicit_tma(const __grid_consta
                 c = over_h<real>((real)K.d2z * T(3, 0, 0, 0), K.hz, K.ihz, K.pow2);
             }
             b = -(a + c);
-            const real az = a * vz[2] + b * vz[3] + c * vz[4];
+            const real az = a * qzm + b * qx[3] + c * qzp;
             const real diff = alpha * (ax + ay + az);
             real S;
             if (VAR == VC) {

@@ -149,14 +149,28 @@ __global__ void __launch_bounds__(FFT_THREADS) k_dct_fft(FftLines d, const real*
     const real* gin = in + a * d.sa_in + b0 * d.sb_in;
     real* gout = out + a * d.sa_out + b0 * d.sb_out;
 
-    // ---- load: line l of the tile -> pair l/2, real (even l) or imaginary part
-    for (int e = tid; e < TL * N; e += FFT_THREADS) {
-        int l, p;
-        if (CONTIG) { l = e / N; p = e % N; } else { p = e / TL; l = e % TL; }
-        const real v = CONTIG ? gin[(long)l * d.sb_in + p] : gin[l + (long)p * d.se_in];
-        const int n = KIND == 0 ? mperm<N>(p) : p;
-        real* slot = &C[(l >> 1) * ROW + fslot<N>(n)].re;
-        slot[l & 1] = v;
+    // ---- load: line l of the tile -> pair l/2, real (even l) or imaginary
+    // part; all of a thread's loads are issued before the first store to
+    // shared memory (TL*N/FFT_THREADS = N/8 of them), so they overlap
+    constexpr int LPT = TL * N / FFT_THREADS;
+    {
+        real v[LPT];
+#pragma unroll
+        for (int t = 0; t < LPT; ++t) {
+            const int e = tid + t * FFT_THREADS;
+            int l, p;
+            if (CONTIG) { l = e / N; p = e % N; } else { p = e / TL; l = e % TL; }
+            v[t] = CONTIG ? gin[(long)l * d.sb_in + p] : gin[l + (long)p * d.se_in];
+        }
+#pragma unroll
+        for (int t = 0; t < LPT; ++t) {
+            const int e = tid + t * FFT_THREADS;
+            int l, p;
+            if (CONTIG) { l = e / N; p = e % N; } else { p = e / TL; l = e % TL; }
+            const int n = KIND == 0 ? mperm<N>(p) : p;
+            real* slot = &C[(l >> 1) * ROW + fslot<N>(n)].re;
+            slot[l & 1] = v[t];
+        }
     }
     __syncthreads();
 
@@ -240,6 +254,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_dct_fft(FftLines d, const real*
 
     // ---- store: DCT-II in natural order; DCT-III through the inverse reordering
     const real sc = (real)d.scale;
+#pragma unroll 8
     for (int e = tid; e < TL * N; e += FFT_THREADS) {
         int l, p;
         if (CONTIG) { l = e / N; p = e % N; } else { p = e / TL; l = e % TL; }
