@@ -48,6 +48,9 @@ extern "C" {
 #define PLLGPU_MIXED 1     /* FP32 state, WENO/stress/ADI in FP32, split-TF32
                               tensor-core DCT, FP64 Poisson mode solve and
                               FP64 reductions                                  */
+#define PLLGPU_MIXED64 2   /* FP64 state and FP64 arithmetic except the WENO5
+                              nonlinear weights, evaluated in FP32 from the
+                              FP64 divided differences                         */
 
 /* run parameters: the values of param.input that the step reads
  * (input() pllcart3d.c:271-350); M = Vratio, Vnorm = 0 (L400-403) */
@@ -56,9 +59,10 @@ typedef struct pllgpu_params {
     int nmvp;              /* Nmvp: 0 mu = exp(M c), 1 non-monotonic law      */
     double X1, X2, Y1, Y2, Z1, Z2;
     double Re, Pe, Vratio, Fx, Fy, CFLmax, Timestep, Mum, Lambda;
-    int precision;         /* PLLGPU_FP64 or PLLGPU_MIXED                      */
+    int precision;         /* PLLGPU_FP64, PLLGPU_MIXED or PLLGPU_MIXED64      */
     int exact_dct;         /* 1: DCT sums in sequential order (bitwise with
-                              the CPU restatement), and in the precision form
+                              the CPU restatement; FP64: the reference's
+                              operation order throughout), and in the precision form
                               every line / mode solve the sequential Thomas
                               sweep; 0: tensor-core DCT, and in the precision
                               form the partitioned line solves and, with the

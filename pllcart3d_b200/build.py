@@ -36,6 +36,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17",
 # order, so no multiply-add is contracted there; the FP64 form (form_f64.cu)
 # and the precision form's FP32 kernels (form_f32.cu) are free to contract.
 CU_SOURCES = {"runtime.cu": "--fmad=false", "form_f64.cu": "--fmad=true", "form_f64x.cu": "--fmad=false",
+              "form_f64m.cu": "--fmad=true",
               "form_f32.cu": "--fmad=true", "primitives.cu": "--fmad=false",
               "noalloc.cu": "--fmad=false", "io.cu": "--fmad=false",
               "wave.cu": "--fmad=false", "ensemble.cu": "--fmad=false"}

@@ -73,14 +73,17 @@ __global__ void __launch_bounds__(128) k_viscosity(Geo G, Rng R, Consts K, int n
     }
 }
 
-// The precision form's exponential law on cell pairs (k, k+32) with packed
-// FP32x2 arithmetic (the averages and exponents; __expf per value), walking
+// The exponential law on cell pairs (k, k+32): the precision form with
+// packed FP32x2 arithmetic (the averages and exponents; __expf per value),
+// the FP64 forms with FP64 pairs and exp(); walking
 // VISC_NI planes as k_viscosity.  A second cell past NZ reads the slack past
 // the array and stores nothing.  Grid: x over k in tiles of 64.
-__global__ void __launch_bounds__(128) k_viscosity2(Geo G, Rng R, Consts K, const float* __restrict__ cn,
-                                                    float* __restrict__ mc, float* __restrict__ mxy,
-                                                    float* __restrict__ mxz, float* __restrict__ myz)
+template <typename real>
+__global__ void __launch_bounds__(128) k_viscosity2(Geo G, Rng R, Consts K, const real* __restrict__ cn,
+                                                    real* __restrict__ mc, real* __restrict__ mxy,
+                                                    real* __restrict__ mxz, real* __restrict__ myz)
 {
+    using T2 = typename PairOf<real>::type;
     const int k = blockIdx.x * (2 * EP_DK) + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (k >= G.NZ || j >= G.NY) return;
@@ -91,34 +94,35 @@ __global__ void __launch_bounds__(128) k_viscosity2(Geo G, Rng R, Consts K, cons
     const bool jxy = (j >= R.js) & (j <= R.je + 1), jin = (j >= R.js) & (j <= R.je);
     const bool kin_a = (k >= R.ks) & (k <= R.ke), kxz_a = (k >= R.ks) & (k <= R.ke + 1);
     const bool kin_b = live_b & (kb <= R.ke), kxz_b = live_b & (kb <= R.ke + 1);
-    const f2 q = S2(0.25f), M = S2((float)K.M), Vn = S2((float)K.Vnorm);
-    auto law = [&](f2 c) {
-        const f2 t = M * (c - Vn);
-        return F2(__expf(t.v.x), __expf(t.v.y));
+    const T2 q = S2((real)0.25), M = S2((real)K.M), Vn = S2((real)K.Vnorm);
+    auto law = [&](T2 c) {
+        const T2 t = M * (c - Vn);
+        if constexpr (sizeof(real) == 4) return mk2(__expf(t.v.x), __expf(t.v.y));
+        else return mk2(exp(t.v.x), exp(t.v.y));
     };
     long id = (long)i0 * sx + (long)j * sy + k;
-    f2 p0 = ld2(cn, id - sx), py = ld2(cn, id - sx - sy), pz = ld2(cn, id - sx - 1);
+    T2 p0 = ld2(cn, id - sx), py = ld2(cn, id - sx - sy), pz = ld2(cn, id - sx - 1);
 #pragma unroll
     for (int t = 0; t < VISC_NI; ++t, id += sx) {
         const int i = i0 + t;
         if (i > R.ie + 1) break;
-        const f2 c0 = ld2(cn, id), cy = ld2(cn, id - sy), cz = ld2(cn, id - 1), cyz = ld2(cn, id - sy - 1);
-        const f2 vc = law(c0);
+        const T2 c0 = ld2(cn, id), cy = ld2(cn, id - sy), cz = ld2(cn, id - 1), cyz = ld2(cn, id - sy - 1);
+        const T2 vc = law(c0);
         mc[id] = vc.v.x;
         if (live_b) mc[id + EP_DK] = vc.v.y;
         const bool in_i = (i >= R.is), in_i2 = (i <= R.ie);
         if (in_i & jxy) {
-            const f2 v = law(q * (py + cy + p0 + c0));
+            const T2 v = law(q * (py + cy + p0 + c0));
             if (kin_a) mxy[id] = v.v.x;
             if (kin_b) mxy[id + EP_DK] = v.v.y;
         }
         if (in_i & jin) {
-            const f2 v = law(q * (pz + cz + p0 + c0));
+            const T2 v = law(q * (pz + cz + p0 + c0));
             if (kxz_a) mxz[id] = v.v.x;
             if (kxz_b) mxz[id + EP_DK] = v.v.y;
         }
         if (in_i & in_i2 & jxy) {
-            const f2 v = law(q * (cyz + cz + cy + c0));
+            const T2 v = law(q * (cyz + cz + cy + c0));
             if (kxz_a) myz[id] = v.v.x;
             if (kxz_b) myz[id + EP_DK] = v.v.y;
         }
@@ -219,31 +223,33 @@ __global__ void __launch_bounds__(512) k_flux(Geo G, Rng Ru, Consts K, const rea
 // cell past ke reads the slack past the arrays and stores nothing.
 constexpr int DIV_NI = 4;
 
-__global__ void __launch_bounds__(128) k_div_rhs2(Geo G, Rng R, Consts K, const float* __restrict__ u,
-                                                  const float* __restrict__ v, const float* __restrict__ w,
-                                                  float* __restrict__ rhs, const double* __restrict__ scal,
+template <typename real>
+__global__ void __launch_bounds__(128) k_div_rhs2(Geo G, Rng R, Consts K, const real* __restrict__ u,
+                                                  const real* __restrict__ v, const real* __restrict__ w,
+                                                  real* __restrict__ rhs, const double* __restrict__ scal,
                                                   double alpha)
 {
+    using T2 = typename PairOf<real>::type;
     const int k = R.ks + blockIdx.x * (2 * EP_DK) + threadIdx.x;
     const int j = R.js + blockIdx.y * blockDim.y + threadIdx.y;
     if (k > R.ke || j > R.je) return;
     const bool live_b = k + EP_DK <= R.ke;
     const int i0 = R.is + blockIdx.z * DIV_NI;
     const long sx = G.sx, sy = G.sy;
-    const f2 ihx = S2((float)K.ihx), ihy = S2((float)K.ihy), ihz = S2((float)K.ihz);
-    const f2 fac = S2((float)(K.Re / (scal[S_DT] * alpha)));
+    const T2 ihx = S2((real)K.ihx), ihy = S2((real)K.ihy), ihz = S2((real)K.ihz);
+    const T2 fac = S2((real)(K.Re / (scal[S_DT] * alpha)));
     const long nj = R.je - R.js + 1, nkk = R.ke - R.ks + 1;
     long id = (long)i0 * sx + (long)j * sy + k;
-    f2 u0 = ld2(u, id);
+    T2 u0 = ld2(u, id);
 #pragma unroll
     for (int t = 0; t < DIV_NI; ++t, id += sx) {
         const int i = i0 + t;
         if (i > R.ie) break;
-        const f2 u1 = ld2(u, id + sx);
-        const f2 dvx = (u1 - u0) * ihx;
-        const f2 dvy = (ld2(v, id + sy) - ld2(v, id)) * ihy;
-        const f2 dvz = (ld2(w, id + 1) - ld2(w, id)) * ihz;
-        const f2 r = fac * (dvx + dvy + dvz);
+        const T2 u1 = ld2(u, id + sx);
+        const T2 dvx = (u1 - u0) * ihx;
+        const T2 dvy = (ld2(v, id + sy) - ld2(v, id)) * ihy;
+        const T2 dvz = (ld2(w, id + 1) - ld2(w, id)) * ihz;
+        const T2 r = fac * (dvx + dvy + dvz);
         const long c = ((long)(i - R.is) * nj + (j - R.js)) * nkk + (k - R.ks);
         rhs[c] = r.v.x;
         if (live_b) rhs[c + EP_DK] = r.v.y;
@@ -709,31 +715,37 @@ __global__ void __launch_bounds__(128) k_project(Geo G, Rng Rg, Rng Ru, Rng Rv, 
 // second cell's are the first's plus 128 bytes) and their add / multiply /
 // fma instructions.  A second cell past ke reads the slack past the arrays'
 // ends and stores nothing.  Grid: x over k in tiles of 64 (blockDim.x 32).
-template <int VAR>
-__device__ __forceinline__ f2 pg_update2(const Consts& K, const Geo& G, const float* __restrict__ phi,
-                                         const MuPtrs<float>& mu, long id, f2 fac, f2 pold)
+template <int VAR, typename real>
+__device__ __forceinline__ typename PairOf<real>::type pg_update2(const Consts& K, const Geo& G,
+                                                                  const real* __restrict__ phi,
+                                                                  const MuPtrs<real>& mu, long id,
+                                                                  typename PairOf<real>::type fac,
+                                                                  typename PairOf<real>::type pold)
 {
+    using T2 = typename PairOf<real>::type;
     const long sx = G.sx, sy = G.sy;
     const long so = VAR == VU ? sx : VAR == VV ? sy : 1;
-    const f2 ih = S2((float)(VAR == VU ? K.ihx : VAR == VV ? K.ihy : K.ihz));
+    const T2 ih = S2((real)(VAR == VU ? K.ihx : VAR == VV ? K.ihy : K.ihz));
     auto gp = [&](long p) { return (ld2(phi, p) - ld2(phi, p - so)) * ih; };
-    f2 a, b, c;
-    const f2 g0 = gp(id);
-    acoef2<VAR, 0>(K, G, mu, id, a, b, c);
-    const f2 pxx = fma2(c, gp(id + sx), fma2(b, g0, a * gp(id - sx)));
-    acoef2<VAR, 1>(K, G, mu, id, a, b, c);
-    const f2 pyy = fma2(c, gp(id + sy), fma2(b, g0, a * gp(id - sy)));
-    acoef2<VAR, 2>(K, G, mu, id, a, b, c);
-    const f2 pzz = fma2(c, gp(id + 1), fma2(b, g0, a * gp(id - 1)));
+    T2 a, b, c;
+    const T2 g0 = gp(id);
+    acoef2<VAR, 0, real>(K, G, mu, id, a, b, c);
+    const T2 pxx = fma2(c, gp(id + sx), fma2(b, g0, a * gp(id - sx)));
+    acoef2<VAR, 1, real>(K, G, mu, id, a, b, c);
+    const T2 pyy = fma2(c, gp(id + sy), fma2(b, g0, a * gp(id - sy)));
+    acoef2<VAR, 2, real>(K, G, mu, id, a, b, c);
+    const T2 pzz = fma2(c, gp(id + 1), fma2(b, g0, a * gp(id - 1)));
     return pold + g0 - fac * (pyy + pxx + pzz);
 }
 
-__global__ void __launch_bounds__(128, 16) k_project2(Geo G, Rng Rg, Rng Ru, Rng Rv, Rng Rw, Consts K,
-        float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
-        float* __restrict__ pgu, float* __restrict__ pgv, float* __restrict__ pgw,
-        const float* __restrict__ phi, MuPtrs<float> mu, const double* __restrict__ scal,
+template <typename real>
+__global__ void __launch_bounds__(128, sizeof(real) == 4 ? 16 : 8) k_project2(Geo G, Rng Rg, Rng Ru, Rng Rv, Rng Rw,
+        Consts K, real* __restrict__ u, real* __restrict__ v, real* __restrict__ w,
+        real* __restrict__ pgu, real* __restrict__ pgv, real* __restrict__ pgw,
+        const real* __restrict__ phi, MuPtrs<real> mu, const double* __restrict__ scal,
         double alpha, int do_correct, int do_ghosts, int do_pg)
 {
+    using T2 = typename PairOf<real>::type;
     const int k = Rg.ks + blockIdx.x * (2 * EP_DK) + threadIdx.x;
     const int j = Rg.js + blockIdx.y * blockDim.y + threadIdx.y;
     const int i = Rg.is + blockIdx.z;
@@ -751,7 +763,7 @@ __global__ void __launch_bounds__(128, 16) k_project2(Geo G, Rng Rg, Rng Ru, Rng
     const bool ghost_i = (i <= Rg.ie);
 
     // ghost copies of one cell (k index kk, values after correction)
-    auto ghosts = [&](long c, int kk, float uval, float vval, float wval) {
+    auto ghosts = [&](long c, int kk, real uval, real vval, real wval) {
         if (kk == Rg.ks) { u[c - 1] = uval; v[c - 1] = vval; }
         if (kk == Rg.ke) { u[c + 1] = uval; v[c + 1] = vval; }
         if (j == Rg.js) { u[c - sy] = -uval; w[c - sy] = -wval; }
@@ -760,16 +772,16 @@ __global__ void __launch_bounds__(128, 16) k_project2(Geo G, Rng Rg, Rng Ru, Rng
     };
 
     if (do_correct) {
-        const f2 fac = S2((float)(dt * alpha / K.Re));
-        f2 uval = ld2(u, id), vval = S2(0.f), wval = S2(0.f);
+        const T2 fac = S2((real)(dt * alpha / K.Re));
+        T2 uval = ld2(u, id), vval = S2((real)0), wval = S2((real)0);
         if (ghost_i) {
             vval = ld2(v, id);
             wval = ld2(w, id);
         }
-        const f2 p0 = ld2(phi, id);
-        const f2 vn = vval - fac * ((p0 - ld2(phi, id - sy)) * S2((float)K.ihy));
-        const f2 wn = wval - fac * ((p0 - ld2(phi, id - 1)) * S2((float)K.ihz));
-        const f2 un = uval - fac * ((p0 - ld2(phi, id - sx)) * S2((float)K.ihx));
+        const T2 p0 = ld2(phi, id);
+        const T2 vn = vval - fac * ((p0 - ld2(phi, id - sy)) * S2((real)K.ihy));
+        const T2 wn = wval - fac * ((p0 - ld2(phi, id - 1)) * S2((real)K.ihz));
+        const T2 un = uval - fac * ((p0 - ld2(phi, id - sx)) * S2((real)K.ihx));
         if (inv_a) { v[id] = vn.v.x; vval.v.x = vn.v.x; }
         if (inv_b) { v[id + EP_DK] = vn.v.y; vval.v.y = vn.v.y; }
         if (inw_a) { w[id] = wn.v.x; wval.v.x = wn.v.x; }
@@ -777,7 +789,7 @@ __global__ void __launch_bounds__(128, 16) k_project2(Geo G, Rng Rg, Rng Ru, Rng
         if (inu_a) { u[id] = un.v.x; uval.v.x = un.v.x; }
         if (inu_b) { u[id + EP_DK] = un.v.y; uval.v.y = un.v.y; }
         if (i == Ru.ie + 1 && j >= Ru.js) {
-            const float def = (float)scal[S_DEFICIT];
+            const real def = (real)scal[S_DEFICIT];
             if (k >= Ru.ks) u[id] = uval.v.x + def;
             if (live_b) u[id + EP_DK] = uval.v.y + def;
         }
@@ -791,19 +803,19 @@ __global__ void __launch_bounds__(128, 16) k_project2(Geo G, Rng Rg, Rng Ru, Rng
     }
 
     if (do_pg) {
-        const f2 fac = S2((float)(0.5 * dt * alpha));
+        const T2 fac = S2((real)(0.5 * dt * alpha));
         if (inv_a | inv_b) {
-            const f2 r = pg_update2<VV>(K, G, phi, mu, id, fac, ld2(pgv, id));
+            const T2 r = pg_update2<VV, real>(K, G, phi, mu, id, fac, ld2(pgv, id));
             if (inv_a) pgv[id] = r.v.x;
             if (inv_b) pgv[id + EP_DK] = r.v.y;
         }
         if (inu_a | inu_b) {
-            const f2 r = pg_update2<VU>(K, G, phi, mu, id, fac, ld2(pgu, id));
+            const T2 r = pg_update2<VU, real>(K, G, phi, mu, id, fac, ld2(pgu, id));
             if (inu_a) pgu[id] = r.v.x;
             if (inu_b) pgu[id + EP_DK] = r.v.y;
         }
         if (inw_a | inw_b) {
-            const f2 r = pg_update2<VW>(K, G, phi, mu, id, fac, ld2(pgw, id));
+            const T2 r = pg_update2<VW, real>(K, G, phi, mu, id, fac, ld2(pgw, id));
             if (inw_a) pgw[id] = r.v.x;
             if (inw_b) pgw[id + EP_DK] = r.v.y;
         }

@@ -21,6 +21,15 @@ void form_diag_f64(pllgpu_ctx* c);
 void form_diag_f32(pllgpu_ctx* c);
 bool form_alloc_f64(pllgpu_ctx* c);
 bool form_alloc_f32(pllgpu_ctx* c);
+// the FP64 form with FP32 WENO5 weights (form_f64m.cu)
+void form_enqueue_step_f64m(pllgpu_ctx* c);
+int form_start_f64m(pllgpu_ctx* c);
+int form_resume_f64m(pllgpu_ctx* c);
+int form_routine_f64m(pllgpu_ctx* c, int routine, const double* in, double* out);
+int form_materialize_f64m(pllgpu_ctx* c);
+void* form_field_ptr_f64m(pllgpu_ctx* c, int f);
+void form_diag_f64m(pllgpu_ctx* c);
+bool form_alloc_f64m(pllgpu_ctx* c);
 // the exact FP64 form (form_f64x.cu)
 void form_enqueue_step_f64x(pllgpu_ctx* c);
 int form_start_f64x(pllgpu_ctx* c);

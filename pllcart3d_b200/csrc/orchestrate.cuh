@@ -114,59 +114,69 @@ void launch_explicit(pllgpu_ctx* ctx, const real* un, const real* vn, const real
     mark(ctx, lab[VAR]);
 }
 
-// the precision form's segmented solve along x (AXIS 0) or y (AXIS 1): lines
-// of P * RS rows or one fewer, P = 16 segments of RS in {4, 8, 16, 32} rows;
-// false: not applicable.  (32 segments of 16 rows for 512-row lines measured
-// slower: at 1024 threads a block spills its 16-row registers.)
-template <int VAR, int AXIS, int P, int RS>
-void line_seg(pllgpu_ctx* ctx, const Rng& R, const XsweepArgs<float>& X, int n)
+// the precision form's segmented solve along x (AXIS 0) or y (AXIS 1):
+// lines of P * RS rows or one fewer, P = 16 segments of RS rows, RS in
+// {4, 8, 16, 32} ({4, 8, 16} for an FP64 instantiation: a thread holds its
+// segment's rows in registers); false: not applicable.  (32 segments of
+// 16 rows for 512-row lines measured slower in FP32: at 1024 threads a block
+// spills its 16-row registers.)
+template <int VAR, int AXIS, int P, int RS, typename real>
+void line_seg(pllgpu_ctx* ctx, const Rng& R, const XsweepArgs<real>& X, int n)
 {
     const dim3 grid((nk(R) + 31) / 32, AXIS == 0 ? nj(R) : ni(R)), blk(32 * P);
-    constexpr size_t smem = line_seg_smem<VAR, AXIS, P, RS>();
+    constexpr size_t smem = line_seg_smem<VAR, AXIS, P, RS, real>();
     if (n == P * RS)
-        k_line_seg<VAR, AXIS, P, RS, true><<<grid, blk, smem, ctx->st>>>(ctx->G, R, ctx->K, X);
+        k_line_seg<VAR, AXIS, P, RS, true, real><<<grid, blk, smem, ctx->st>>>(ctx->G, R, ctx->K, X);
     else
-        k_line_seg<VAR, AXIS, P, RS, false><<<grid, blk, smem, ctx->st>>>(ctx->G, R, ctx->K, X);
+        k_line_seg<VAR, AXIS, P, RS, false, real><<<grid, blk, smem, ctx->st>>>(ctx->G, R, ctx->K, X);
 }
 
-template <int VAR, int AXIS>
-bool launch_line_seg(pllgpu_ctx* ctx, const Rng& R, const XsweepArgs<float>& X)
+template <int VAR, int AXIS, typename real>
+bool launch_line_seg(pllgpu_ctx* ctx, const Rng& R, const XsweepArgs<real>& X)
 {
     if (ctx->P.exact_dct || ctx->nelem >= (1L << 31)) return false;
     const int n = AXIS == 0 ? ni(R) : nj(R);
     constexpr int p = 16;
     const int rs = (n + p - 1) / p;   // rows per segment
-    if (rs != 4 && rs != 8 && rs != 16 && rs != 32) return false;
+    constexpr bool f32 = std::is_same<real, float>::value;
+    if (rs != 4 && rs != 8 && rs != 16 && !(f32 && rs == 32)) return false;
     if (n != p * rs) {
         // one row short: the kernel loads the row past the line (and the
         // viscosity family one beyond it), which must lie in the padded box
         const int start = AXIS == 0 ? R.is : R.js, top = AXIS == 0 ? ctx->G.NX - 1 : ctx->G.NY - 1;
         if (n != p * rs - 1 || start + p * rs + LineCoef<VAR, AXIS>::off > top) return false;
     }
-    if (rs == 4) line_seg<VAR, AXIS, p, 4>(ctx, R, X, n);
-    else if (rs == 8) line_seg<VAR, AXIS, p, 8>(ctx, R, X, n);
-    else if (rs == 16) line_seg<VAR, AXIS, p, 16>(ctx, R, X, n);
-    else line_seg<VAR, AXIS, p, 32>(ctx, R, X, n);
+    if (rs == 4) line_seg<VAR, AXIS, p, 4, real>(ctx, R, X, n);
+    else if (rs == 8) line_seg<VAR, AXIS, p, 8, real>(ctx, R, X, n);
+    else if (rs == 16) line_seg<VAR, AXIS, p, 16, real>(ctx, R, X, n);
+    else if constexpr (f32) line_seg<VAR, AXIS, p, 32, real>(ctx, R, X, n);
     return true;
 }
 
-// shared-memory limits of the segmented solves (the tiles pass 48 KB for
-// 16 and 32 rows per segment)
-template <int VAR, int AXIS, int P, int RS>
+// shared-memory opt-in of the segmented solves (static separator arrays and
+// dynamic row tiles together pass the 48 KB default: FP32 from 16 rows per
+// segment, FP64 from 4)
+template <int VAR, int AXIS, int P, int RS, typename real>
 void line_seg_attr()
 {
-    const int b = (int)line_seg_smem<VAR, AXIS, P, RS>();
-    cudaFuncSetAttribute(k_line_seg<VAR, AXIS, P, RS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    cudaFuncSetAttribute(k_line_seg<VAR, AXIS, P, RS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    const int b = (int)line_seg_smem<VAR, AXIS, P, RS, real>();
+    cudaFuncSetAttribute(k_line_seg<VAR, AXIS, P, RS, true, real>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    cudaFuncSetAttribute(k_line_seg<VAR, AXIS, P, RS, false, real>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
 }
 
-template <int VAR>
+template <int VAR, typename real>
 void line_seg_attrs()
 {
-    line_seg_attr<VAR, 0, 16, 16>();
-    line_seg_attr<VAR, 0, 16, 32>();
-    line_seg_attr<VAR, 1, 16, 16>();
-    line_seg_attr<VAR, 1, 16, 32>();
+    line_seg_attr<VAR, 0, 16, 4, real>();
+    line_seg_attr<VAR, 1, 16, 4, real>();
+    line_seg_attr<VAR, 0, 16, 8, real>();
+    line_seg_attr<VAR, 0, 16, 16, real>();
+    line_seg_attr<VAR, 1, 16, 8, real>();
+    line_seg_attr<VAR, 1, 16, 16, real>();
+    if constexpr (std::is_same<real, float>::value) {
+        line_seg_attr<VAR, 0, 16, 32, real>();
+        line_seg_attr<VAR, 1, 16, 32, real>();
+    }
 }
 
 template <typename real, int VAR>
@@ -194,8 +204,12 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
     bool ydone = false;
     if constexpr (std::is_same<real, float>::value) {
         // the precision form's partitioned solves: segmented when the line
-        // length allows, else for concentration the warp solve of short lines
-        ydone = launch_line_seg<VAR, 1>(ctx, R, X);
+        // length allows, else for concentration the warp solve of short
+        // lines.  (In FP64 a segment's rows fill a 512-thread block's
+        // registers, one block per SM, and the segmented y solve measured
+        // slower than the prefetching sweep: 1.12 against 1.00 ms per
+        // variable and step at 512x256x256.)
+        ydone = launch_line_seg<VAR, 1, real>(ctx, R, X);
         if (!ydone && VAR == VC && nj(R) <= ZP_MAX && nj(R) >= 2 * (ZP_MAX / 32) && !ctx->P.exact_dct) {
             k_adi_y_part<VAR, float><<<dim3((nk(R) + 31) / 32, ni(R)), 256, adi_y_part_smem<float>(), ctx->st>>>(
                 ctx->G, R, ctx->K, X.mu, B.S, ctx->scal, alpha);
@@ -221,7 +235,7 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
     }
     mark(ctx, lz[VAR]);
     bool xdone = false;
-    if constexpr (std::is_same<real, float>::value) xdone = launch_line_seg<VAR, 0>(ctx, R, X);
+    if constexpr (std::is_same<real, float>::value) xdone = launch_line_seg<VAR, 0, real>(ctx, R, X);
     if (!xdone)
         k_line_pf<VAR, 0, real><<<dim3((nk(R) + lb - 1) / lb, nj(R)), lb, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
     mark(ctx, lx[VAR]);
@@ -231,12 +245,12 @@ template <typename real>
 void launch_viscosity(pllgpu_ctx* ctx, const real* cn, MuPtrs<real> m, int law = -1)
 {
     dim3 blk(32, 4);
-    if constexpr (std::is_same<real, float>::value) {
+    if constexpr (std::is_same<real, float>::value || !PLL_FP64_EXACT) {
         if ((law < 0 ? ctx->P.nmvp : law) == 0) {   // the exponential law on cell pairs
             const dim3 grid((ctx->G.NZ + 2 * EP_DK - 1) / (2 * EP_DK), (ctx->G.NY + blk.y - 1) / blk.y,
                             (ni(ctx->Rg) + 2 + VISC_NI - 1) / VISC_NI);
-            k_viscosity2<<<grid, blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->K, cn, (float*)m.cell, (float*)m.xy,
-                                                    (float*)m.xz, (float*)m.yz);
+            k_viscosity2<real><<<grid, blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->K, cn, (real*)m.cell, (real*)m.xy,
+                                                          (real*)m.xz, (real*)m.yz);
             mark(ctx, "viscosity");
             return;
         }
@@ -432,10 +446,10 @@ void launch_project(pllgpu_ctx* ctx, double alpha, int correct, int ghosts, int 
     Bufs<real>& B = bufs<real>(ctx);
     const MuPtrs<real> mu = mu_new<real>(ctx);
     dim3 blk(32, 4);
-    if constexpr (std::is_same<real, float>::value) {
+    if constexpr (std::is_same<real, float>::value || !PLL_FP64_EXACT) {
         const dim3 grid((nk(ctx->Rg) + 2 * EP_DK - 1) / (2 * EP_DK), (nj(ctx->Rg) + blk.y - 1) / blk.y,
                         ni(ctx->Rg) + 1);
-        k_project2<<<grid, blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->Rv[VU], ctx->Rv[VV], ctx->Rv[VW], ctx->K,
+        k_project2<real><<<grid, blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->Rv[VU], ctx->Rv[VV], ctx->Rv[VW], ctx->K,
                                               q_new<real>(ctx, VU), q_new<real>(ctx, VV), q_new<real>(ctx, VW),
                                               B.pg[VU], B.pg[VV], B.pg[VW], B.phi, mu, ctx->scal, alpha, correct,
                                               ghosts, pgu);
@@ -455,11 +469,11 @@ void launch_div(pllgpu_ctx* ctx, int mode, double alpha)
 {
     Bufs<real>& B = bufs<real>(ctx);
     dim3 blk(32, 4);
-    if constexpr (std::is_same<real, float>::value) {
-        if (mode == 0) {   // the precision form's right-hand side on cell pairs
+    if constexpr (std::is_same<real, float>::value || !PLL_FP64_EXACT) {
+        if (mode == 0) {   // the right-hand side on cell pairs
             const dim3 grid((nk(ctx->Rg) + 2 * EP_DK - 1) / (2 * EP_DK), (nj(ctx->Rg) + blk.y - 1) / blk.y,
                             (ni(ctx->Rg) + DIV_NI - 1) / DIV_NI);
-            k_div_rhs2<<<grid, blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->K, q_new<real>(ctx, VU), q_new<real>(ctx, VV),
+            k_div_rhs2<real><<<grid, blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->K, q_new<real>(ctx, VU), q_new<real>(ctx, VV),
                                                   q_new<real>(ctx, VW), B.dct1, ctx->scal, alpha);
             mark(ctx, "div_rhs");
             return;
@@ -939,10 +953,12 @@ bool alloc_state(pllgpu_ctx* c)
                              (int)adi_y_part_smem<float>());
         cudaFuncSetAttribute(k_adi_y_part<VW, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)adi_y_part_smem<float>());
-        line_seg_attrs<VC>();
-        line_seg_attrs<VU>();
-        line_seg_attrs<VV>();
-        line_seg_attrs<VW>();
+    }
+    if constexpr (std::is_same<real, float>::value) {
+        line_seg_attrs<VC, real>();
+        line_seg_attrs<VU, real>();
+        line_seg_attrs<VV, real>();
+        line_seg_attrs<VW, real>();
     }
     cudaFuncSetAttribute(k_adi_z_tiled<VC, real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)adi_z_smem_bytes<VC, real>());

@@ -39,14 +39,18 @@
 
 using namespace pll;
 
+// one entry point of the context's form: the precision form (FP32 state),
+// the exact FP64 form (exact_dct), the FP64 form with FP32 WENO weights, or
+// the FP64 form
+#define FORM_CALL(c, fn, ...)                                                                          \
+    ((c)->mixed                                 ? fn##_f32(__VA_ARGS__)                              \
+     : (c)->P.exact_dct                         ? fn##_f64x(__VA_ARGS__)                             \
+     : (c)->P.precision == PLLGPU_MIXED64       ? fn##_f64m(__VA_ARGS__)                             \
+                                                : fn##_f64(__VA_ARGS__))
+
 namespace pll {
 
-void enqueue_step_any(pllgpu_ctx* ctx)
-{
-    if (ctx->mixed) form_enqueue_step_f32(ctx);
-    else if (ctx->P.exact_dct) form_enqueue_step_f64x(ctx);
-    else form_enqueue_step_f64(ctx);
-}
+void enqueue_step_any(pllgpu_ctx* ctx) { FORM_CALL(ctx, form_enqueue_step, ctx); }
 
 namespace {
 
@@ -120,7 +124,7 @@ namespace pll {
 
 static int materialize_t_any(pllgpu_ctx* ctx)
 {
-    return ctx->mixed ? form_materialize_f32(ctx) : ctx->P.exact_dct ? form_materialize_f64x(ctx) : form_materialize_f64(ctx);
+    return FORM_CALL(ctx, form_materialize, ctx);
 }
 
 int materialize(pllgpu_ctx* ctx)
@@ -140,7 +144,7 @@ void* field_ptr(pllgpu_ctx* ctx, int f, bool for_write)
         if (!for_write) f = new_to_old(f);
         else if (materialize(ctx)) return nullptr;
     }
-    return ctx->mixed ? form_field_ptr_f32(ctx, f) : ctx->P.exact_dct ? form_field_ptr_f64x(ctx, f) : form_field_ptr_f64(ctx, f);
+    return FORM_CALL(ctx, form_field_ptr, ctx, f);
 }
 
 }  // namespace pll
@@ -167,7 +171,8 @@ const char* pllgpu_error_string(int code)
 pllgpu_ctx* pllgpu_create(const pllgpu_params* p, int device)
 {
     if (!p || p->nx < 4 || p->ny < 4 || p->nz < 4) return nullptr;
-    if (p->precision != PLLGPU_FP64 && p->precision != PLLGPU_MIXED) return nullptr;
+    if (p->precision != PLLGPU_FP64 && p->precision != PLLGPU_MIXED && p->precision != PLLGPU_MIXED64)
+        return nullptr;
     pllgpu_ctx* ctx = new pllgpu_ctx();
     ctx->P = *p;
     ctx->dev = device;
@@ -225,7 +230,7 @@ pllgpu_ctx* pllgpu_create(const pllgpu_params* p, int device)
 
     pllgpu_ctx* c = ctx;
     const long ncell = (long)p->nx * p->ny * p->nz;
-    bool ok = ctx->mixed ? form_alloc_f32(c) : ctx->P.exact_dct ? form_alloc_f64x(c) : form_alloc_f64(c);
+    bool ok = FORM_CALL(ctx, form_alloc, c);
     ok = ok && (c->mode_cc = dalloc<double>(c, ncell)) && (c->mode_rr = dalloc<double>(c, ncell)) &&
          (c->lam_y = dalloc<double>(c, p->ny)) && (c->lam_z = dalloc<double>(c, p->nz)) &&
          (c->scal = dalloc<double>(c, S_COUNT)) && (c->work = dalloc<double>(c, 2L * (p->nx + 8))) &&
@@ -353,7 +358,7 @@ int pllgpu_start(pllgpu_ctx* ctx)
     if (!ctx) return PLLGPU_EINVAL;
     CK(cudaSetDevice(ctx->dev));
     if (int e = materialize(ctx)) return e;
-    int e = ctx->mixed ? form_start_f32(ctx) : ctx->P.exact_dct ? form_start_f64x(ctx) : form_start_f64(ctx);
+    int e = FORM_CALL(ctx, form_start, ctx);
     if (e) return e;
     if (int e2 = check_launch(ctx)) return e2;
     CK(cudaStreamSynchronize(ctx->st));
@@ -366,7 +371,7 @@ int pllgpu_resume(pllgpu_ctx* ctx, double tval)
     if (!ctx) return PLLGPU_EINVAL;
     CK(cudaSetDevice(ctx->dev));
     if (int e = materialize(ctx)) return e;
-    int e = ctx->mixed ? form_resume_f32(ctx) : ctx->P.exact_dct ? form_resume_f64x(ctx) : form_resume_f64(ctx);
+    int e = FORM_CALL(ctx, form_resume, ctx);
     if (e) return e;
     ctx->resync_c = true;
     if (int e2 = check_launch(ctx)) return e2;
@@ -547,9 +552,7 @@ int pllgpu_routine(pllgpu_ctx* ctx, int routine, const double* in, double* out)
     CK(cudaSetDevice(ctx->dev));
     if (routine != PLLGPU_R_SUBSTEP)
         if (int e = materialize(ctx)) return e;
-    int e = ctx->mixed ? form_routine_f32(ctx, routine, in, out)
-            : ctx->P.exact_dct ? form_routine_f64x(ctx, routine, in, out)
-                               : form_routine_f64(ctx, routine, in, out);
+    int e = FORM_CALL(ctx, form_routine, ctx, routine, in, out);
     if (e) return e;
     if (int e2 = check_launch(ctx)) return e2;
     CK(cudaStreamSynchronize(ctx->st));
@@ -560,9 +563,7 @@ int pllgpu_diagnostics(pllgpu_ctx* ctx, double* out4)
 {
     if (!ctx || !out4) return PLLGPU_EINVAL;
     CK(cudaSetDevice(ctx->dev));
-    if (ctx->mixed) form_diag_f32(ctx);
-    else if (ctx->P.exact_dct) form_diag_f64x(ctx);
-    else form_diag_f64(ctx);
+    FORM_CALL(ctx, form_diag, ctx);
     if (int e = check_launch(ctx)) return e;
     CK(cudaMemcpyAsync(out4, ctx->diag + 3L * ni(ctx->Rg), sizeof(double) * 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));

@@ -117,7 +117,11 @@ __device__ __forceinline__ real weno5(real v0, real v1, real v2, real v3, real v
     return (a1 / at) * c1 + (a2 / at) * c2 + (a3 / at) * c3;
 }
 
-#if !PLL_FP64_EXACT
+#ifndef PLL_WENO_F32
+#define PLL_WENO_F32 0
+#endif
+
+#if !PLL_FP64_EXACT && !PLL_WENO_F32
 // The FP64 form's WENO5: the same nonlinear weights with one division.  The
 // weights a_i = w_i / e_i^2 (e_i = s_i + eps) enter only through the ratio
 // sum(a_i c_i) / sum(a_i), which is unchanged when every a_i is multiplied
@@ -182,6 +186,18 @@ __device__ __forceinline__ float weno5<float>(float v0, float v1, float v2, floa
     const float a3 = __fdividef(0.3f, (s3 + eps) * (s3 + eps));
     return __fdividef(a1 * c1 + a2 * c2 + a3 * c3, a1 + a2 + a3);
 }
+
+#if !PLL_FP64_EXACT && PLL_WENO_F32
+// The FP64-state form's WENO5: the five FP64 divided differences rounded to
+// FP32 once, the smoothness indicators, weights and weighted sum in FP32
+// (weno5<float>), the result widened back.  Relative error of the derivative
+// ~1e-7; every other operation of the step stays FP64.
+template <>
+__device__ __forceinline__ double weno5<double>(double v0, double v1, double v2, double v3, double v4)
+{
+    return (double)weno5<float>((float)v0, (float)v1, (float)v2, (float)v3, (float)v4);
+}
+#endif
 
 // D2 value an earlier directional pass of the same H*_op call left in its
 // scratch line at index m (pllcart3d.c:1545-1546: D1/D2 are allocated once
@@ -460,6 +476,32 @@ constexpr int EP_DK = 32;   // k distance of a thread's two cells
 
 __device__ __forceinline__ f2 ld2(const float* __restrict__ p, long id) { return F2(p[id], p[id + EP_DK]); }
 
+// the same cell pairs in FP64 (used by the FP64 forms): each operation is
+// two scalar FP64 operations, the pair sharing its addressing
+struct d2 {
+    double2 v;
+};
+__device__ __forceinline__ d2 D2(double a, double b) { return d2{make_double2(a, b)}; }
+__device__ __forceinline__ d2 S2(double a) { return D2(a, a); }
+__device__ __forceinline__ d2 operator+(d2 a, d2 b) { return D2(a.v.x + b.v.x, a.v.y + b.v.y); }
+__device__ __forceinline__ d2 operator*(d2 a, d2 b) { return D2(a.v.x * b.v.x, a.v.y * b.v.y); }
+__device__ __forceinline__ d2 operator-(d2 a, d2 b) { return D2(a.v.x - b.v.x, a.v.y - b.v.y); }
+__device__ __forceinline__ d2 fma2(d2 b, d2 c, d2 a) { return D2(fma(b.v.x, c.v.x, a.v.x), fma(b.v.y, c.v.y, a.v.y)); }
+__device__ __forceinline__ d2 neg2(d2 a) { return D2(-a.v.x, -a.v.y); }
+__device__ __forceinline__ d2 ld2(const double* __restrict__ p, long id) { return D2(p[id], p[id + EP_DK]); }
+__device__ __forceinline__ f2 mk2(float a, float b) { return F2(a, b); }
+__device__ __forceinline__ d2 mk2(double a, double b) { return D2(a, b); }
+
+// the pair type of an arithmetic type
+template <typename real>
+struct PairOf {
+    using type = f2;
+};
+template <>
+struct PairOf<double> {
+    using type = d2;
+};
+
 // packed weno5<float>: the same weights with the approximate divisions per
 // component
 __device__ __forceinline__ f2 weno5_2(f2 v0, f2 v1, f2 v2, f2 v3, f2 v4)
@@ -542,46 +584,48 @@ __device__ __forceinline__ f2 upwind_deriv2(const float* __restrict__ q, const G
     return weno5_2(pick(0, 5), pick(1, 4), pick(2, 3), pick(3, 2), pick(4, 1));
 }
 
-template <int VAR, int AXIS>
-__device__ __forceinline__ void acoef2(const Consts& K, const Geo& G, const MuPtrs<float>& mu, long id, f2& a,
-                                       f2& b, f2& c)
+template <int VAR, int AXIS, typename real>
+__device__ __forceinline__ void acoef2(const Consts& K, const Geo& G, const MuPtrs<real>& mu, long id,
+                                       typename PairOf<real>::type& a, typename PairOf<real>::type& b,
+                                       typename PairOf<real>::type& c)
 {
+    using T2 = typename PairOf<real>::type;
     const long sx = G.sx, sy = G.sy;
-    const f2 ihx = S2((float)K.ihx), ihy = S2((float)K.ihy), ihz = S2((float)K.ihz);
+    const T2 ihx = S2((real)K.ihx), ihy = S2((real)K.ihy), ihz = S2((real)K.ihz);
     if (VAR == VC) {
-        a = c = S2((float)(AXIS == 0 ? K.cdx : AXIS == 1 ? K.cdy : K.cdz));
+        a = c = S2((real)(AXIS == 0 ? K.cdx : AXIS == 1 ? K.cdy : K.cdz));
     } else if (VAR == VU) {
         if (AXIS == 0) {
-            a = S2((float)K.d2x) * ld2(mu.cell, id - sx) * ihx;
-            c = S2((float)K.d2x) * ld2(mu.cell, id) * ihx;
+            a = S2((real)K.d2x) * ld2(mu.cell, id - sx) * ihx;
+            c = S2((real)K.d2x) * ld2(mu.cell, id) * ihx;
         } else if (AXIS == 1) {
-            a = S2((float)K.d1y) * ld2(mu.xy, id) * ihy;
-            c = S2((float)K.d1y) * ld2(mu.xy, id + sy) * ihy;
+            a = S2((real)K.d1y) * ld2(mu.xy, id) * ihy;
+            c = S2((real)K.d1y) * ld2(mu.xy, id + sy) * ihy;
         } else {
-            a = S2((float)K.d1z) * ld2(mu.xz, id) * ihz;
-            c = S2((float)K.d1z) * ld2(mu.xz, id + 1) * ihz;
+            a = S2((real)K.d1z) * ld2(mu.xz, id) * ihz;
+            c = S2((real)K.d1z) * ld2(mu.xz, id + 1) * ihz;
         }
     } else if (VAR == VV) {
         if (AXIS == 0) {
-            a = S2((float)K.d1x) * ld2(mu.xy, id) * ihx;
-            c = S2((float)K.d1x) * ld2(mu.xy, id + sx) * ihx;
+            a = S2((real)K.d1x) * ld2(mu.xy, id) * ihx;
+            c = S2((real)K.d1x) * ld2(mu.xy, id + sx) * ihx;
         } else if (AXIS == 1) {
-            a = S2((float)K.d2y) * ld2(mu.cell, id - sy) * ihy;
-            c = S2((float)K.d2y) * ld2(mu.cell, id) * ihy;
+            a = S2((real)K.d2y) * ld2(mu.cell, id - sy) * ihy;
+            c = S2((real)K.d2y) * ld2(mu.cell, id) * ihy;
         } else {
-            a = S2((float)K.d1z) * ld2(mu.yz, id) * ihz;
-            c = S2((float)K.d1z) * ld2(mu.yz, id + 1) * ihz;
+            a = S2((real)K.d1z) * ld2(mu.yz, id) * ihz;
+            c = S2((real)K.d1z) * ld2(mu.yz, id + 1) * ihz;
         }
     } else {
         if (AXIS == 0) {
-            a = S2((float)K.d1x) * ld2(mu.xz, id) * ihx;
-            c = S2((float)K.d1x) * ld2(mu.xz, id + sx) * ihx;
+            a = S2((real)K.d1x) * ld2(mu.xz, id) * ihx;
+            c = S2((real)K.d1x) * ld2(mu.xz, id + sx) * ihx;
         } else if (AXIS == 1) {
-            a = S2((float)K.d1y) * ld2(mu.yz, id) * ihy;
-            c = S2((float)K.d1y) * ld2(mu.yz, id + sy) * ihy;
+            a = S2((real)K.d1y) * ld2(mu.yz, id) * ihy;
+            c = S2((real)K.d1y) * ld2(mu.yz, id + sy) * ihy;
         } else {
-            a = S2((float)K.d2z) * ld2(mu.cell, id - 1) * ihz;
-            c = S2((float)K.d2z) * ld2(mu.cell, id) * ihz;
+            a = S2((real)K.d2z) * ld2(mu.cell, id - 1) * ihz;
+            c = S2((real)K.d2z) * ld2(mu.cell, id) * ihz;
         }
     }
     b = neg2(a + c);
@@ -1408,17 +1452,24 @@ __global__ void __launch_bounds__(128) k_line_pf(Geo G, Rng R, Consts K, XsweepA
 
 // dynamic shared memory of k_line_seg: the viscosity family's rows (RS + 1
 // per thread, momentum) then the x sweep's q_old rows (RS per thread)
-template <int VAR, int AXIS, int P, int RS>
+template <int VAR, int AXIS, int P, int RS, typename real = float>
 constexpr size_t line_seg_smem()
 {
-    return sizeof(float) * 32 * P * ((VAR != VC ? RS + 1 : 0) + (AXIS == 0 ? RS : 0));
+    return sizeof(real) * 32 * P * ((VAR != VC ? RS + 1 : 0) + (AXIS == 0 ? RS : 0));
 }
 
-__device__ __forceinline__ void ls_cp_async4(float* dst, const float* src)
+// one element global -> shared by cp.async (4 or 8 bytes)
+template <typename real>
+__device__ __forceinline__ void ls_cp_async(real* dst, const real* src)
 {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
-                 "l"(src)
-                 : "memory");
+    if (sizeof(real) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                     "l"(src)
+                     : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                     "l"(src)
+                     : "memory");
 }
 
 // an optimisation barrier on x: later reads cannot reuse values computed
@@ -1426,17 +1477,20 @@ __device__ __forceinline__ void ls_cp_async4(float* dst, const float* src)
 // of holding four per row in registers; a "memory" clobber does the same
 // for the shared-memory rows)
 __device__ __forceinline__ void ls_fresh(float& x) { asm volatile("" : "+f"(x)); }
+__device__ __forceinline__ void ls_fresh(double& x) { asm volatile("" : "+d"(x)); }
 
 // FULL: the line has P * RS rows; else P * RS - 1 and the last
 // segment's last row is an identity row (its loads read the row past the
 // line, which the host checks lies inside the padded box)
-template <int VAR, int AXIS, int P, int RS, bool FULL>
-__global__ void __launch_bounds__(32 * P, RS <= 16 ? 2 : 1) k_line_seg(Geo G, Rng R, Consts K, XsweepArgs<float> A)
+template <int VAR, int AXIS, int P, int RS, bool FULL, typename real = float>
+__global__ void __launch_bounds__(32 * P, (RS <= 16 && sizeof(real) == 4) ? 2 : 1)
+    k_line_seg(Geo G, Rng R, Consts K, XsweepArgs<real> A)
 {
-    __shared__ float eq[4][P][32];       // separator equations
-    __shared__ float tail[3][P][32];     // last interior row of each segment
-    __shared__ float sep[P + 1][32];     // separator values
-    extern __shared__ float ls_dyn[];       // [row][thread] tiles: viscosity, then q_old (x)
+    __shared__ real eq[4][P][32];       // separator equations
+    __shared__ real tail[3][P][32];     // last interior row of each segment
+    __shared__ real sep[P + 1][32];     // separator values
+    extern __shared__ __align__(16) unsigned char ls_raw[];
+    real* ls_dyn = (real*)ls_raw;       // [row][thread] tiles: viscosity, then q_old (x)
     constexpr int LO = Closure<VAR, AXIS>::lo, HI = Closure<VAR, AXIS>::hi;
     constexpr int OFF = LineCoef<VAR, AXIS>::off;
     constexpr int TS = 32 * P;
@@ -1451,45 +1505,45 @@ __global__ void __launch_bounds__(32 * P, RS <= 16 ? 2 : 1) k_line_seg(Geo G, Rn
     const long base = AXIS == 0 ? (long)R.is * G.sx + (long)(R.js + o) * G.sy + k
                                 : (long)(R.is + o) * G.sx + (long)R.js * G.sy + k;
     const long seg = base + (long)(l * RS) * st;
-    const float dt = (float)A.scal[S_DT];
-    const float fac = (float)(0.5 * A.scal[S_DT] * A.alpha);
-    const float* __restrict__ fam = VAR == VC ? nullptr : line_family<VAR, AXIS, float>(A.mu);
-    float* __restrict__ S = A.S;
+    const real dt = (real)A.scal[S_DT];
+    const real fac = (real)(0.5 * A.scal[S_DT] * A.alpha);
+    const real* __restrict__ fam = VAR == VC ? nullptr : line_family<VAR, AXIS, real>(A.mu);
+    real* __restrict__ S = A.S;
     // this thread's row e of the tiles: mym[e * TS], myq[e * TS]
-    float* mym = ls_dyn + threadIdx.x;
-    float* myq = ls_dyn + (VAR != VC ? (RS + 1) * TS : 0) + threadIdx.x;
+    real* mym = ls_dyn + threadIdx.x;
+    real* myq = ls_dyn + (VAR != VC ? (RS + 1) * TS : 0) + threadIdx.x;
 
     if (VAR != VC) {
         if (live) {
-            const float* mp = fam + seg + OFF * st;
+            const real* mp = fam + seg + OFF * st;
 #pragma unroll
-            for (int e = 0; e <= RS; ++e) ls_cp_async4(mym + e * TS, mp + e * st);
+            for (int e = 0; e <= RS; ++e) ls_cp_async<real>(mym + e * TS, mp + e * st);
         } else {
 #pragma unroll
-            for (int e = 0; e <= RS; ++e) mym[e * TS] = 0.f;
+            for (int e = 0; e <= RS; ++e) mym[e * TS] = (real)0;
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
     if (AXIS == 0 && live) {
 #pragma unroll
-        for (int e = 0; e < RS; ++e) ls_cp_async4(myq + e * TS, A.q + seg + e * st);
+        for (int e = 0; e < RS; ++e) ls_cp_async<real>(myq + e * TS, A.q + seg + e * st);
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
-    float rS[RS];
+    real rS[RS];
     {
-        const float* sp = S + seg;
+        const real* sp = S + seg;
 #pragma unroll
-        for (int e = 0; e < RS; ++e) rS[e] = live ? sp[e * st] : 0.f;
+        for (int e = 0; e < RS; ++e) rS[e] = live ? sp[e * st] : (real)0;
     }
 
     // convective outflow value (x): the thread that owns the line's last row
-    float boun = 0.f;
+    real boun = (real)0;
     if (AXIS == 0 && live && last_seg) {
         const long rb = base + (long)n * st;
-        float Hb = -(float)A.scal[S_VBULK] * (A.q[rb] - A.q[rb - st]);
-        Hb = over_h<float>(Hb, K.hx, K.ihx, K.pow2);
+        real Hb = -(real)A.scal[S_VBULK] * (A.q[rb] - A.q[rb - st]);
+        Hb = over_h<real>(Hb, K.hx, K.ihx, K.pow2);
         A.H[rb] = Hb;
-        boun = dt * ((float)A.g * Hb + (float)A.r * A.Hm[rb]);
+        boun = dt * ((real)A.g * Hb + (real)A.r * A.Hm[rb]);
         A.qn[rb] = A.q[rb] + boun;
     }
     if (VAR != VC) {
@@ -1501,31 +1555,31 @@ __global__ void __launch_bounds__(32 * P, RS <= 16 ? 2 : 1) k_line_seg(Geo G, Rn
     // row e of this segment: (la, lb, lc, lr) with the line's closures; la of
     // the line's first row and lc of its last are dropped (the sequential
     // sweep multiplies them by zero)
-    auto row = [&](int e, float& la, float& lb, float& lc, float& lr) {
+    auto row = [&](int e, real& la, real& lb, real& lc, real& lr) {
         if (!FULL && last_seg && e == RS - 1) {
-            la = 0.f;
-            lb = 1.0f;
-            lc = 0.f;
-            lr = 0.f;
+            la = (real)0;
+            lb = (real)1;
+            lc = (real)0;
+            lr = (real)0;
             return;
         }
-        float a, c;
-        line_ac<VAR, AXIS, float>(K, VAR == VC ? 0.f : mym[e * TS], VAR == VC ? 0.f : mym[(e + 1) * TS], a, c);
-        const float b = -(a + c);
+        real a, c;
+        line_ac<VAR, AXIS, real>(K, VAR == VC ? (real)0 : mym[e * TS], VAR == VC ? (real)0 : mym[(e + 1) * TS], a, c);
+        const real b = -(a + c);
         la = -fac * a;
-        lb = 1.0f - fac * b;
+        lb = (real)1 - fac * b;
         lc = -fac * c;
         lr = rS[e];
         if (e == 0 && l == 0) {
             if (LO == 1) lb += la;
             else if (LO == 2) lb -= la;
-            la = 0.f;
+            la = (real)0;
         }
         if (last_seg && e == (FULL ? RS - 1 : RS - 2)) {
             if (AXIS == 0) lr -= lc * boun;
             else if (HI == 1) lb += lc;
             else if (HI == 2) lb -= lc;
-            lc = 0.f;
+            lc = (real)0;
         }
     };
     auto fresh = [&]() {
@@ -1536,16 +1590,16 @@ __global__ void __launch_bounds__(32 * P, RS <= 16 ? 2 : 1) k_line_seg(Geo G, Rn
 
     // interior rows top-down: x_e = rh - ah S_l - ch x_{e+1}; at the last
     // interior row x_{e+1} is the next separator
-    float gL, vL, wL;
+    real gL, vL, wL;
     {
-        float la, lb, lc, lr;
+        real la, lb, lc, lr;
         row(1, la, lb, lc, lr);
-        float ib = __fdividef(1.0f, lb);
-        float ch = lc * ib, rh = lr * ib, ah = la * ib;
+        real ib = rcp_<real>(lb);
+        real ch = lc * ib, rh = lr * ib, ah = la * ib;
 #pragma unroll
         for (int e = 2; e < RS; ++e) {
             row(e, la, lb, lc, lr);
-            ib = __fdividef(1.0f, lb - la * ch);
+            ib = rcp_<real>(lb - la * ch);
             rh = (lr - la * rh) * ib;
             ah = -la * ah * ib;
             ch = lc * ib;
@@ -1556,16 +1610,16 @@ __global__ void __launch_bounds__(32 * P, RS <= 16 ? 2 : 1) k_line_seg(Geo G, Rn
     }
     fresh();
     // bottom-up: x_e = rb - ab S_l - cb S_{l+1} down to the first interior row
-    float g1, v1, w1;
+    real g1, v1, w1;
     {
-        float la, lb, lc, lr;
+        real la, lb, lc, lr;
         row(RS - 1, la, lb, lc, lr);
-        float ib = __fdividef(1.0f, lb);
-        float rb = lr * ib, cb = lc * ib, ab = la * ib;
+        real ib = rcp_<real>(lb);
+        real rb = lr * ib, cb = lc * ib, ab = la * ib;
 #pragma unroll
         for (int e = RS - 2; e >= 1; --e) {
             row(e, la, lb, lc, lr);
-            ib = __fdividef(1.0f, lb - lc * ab);
+            ib = rcp_<real>(lb - lc * ab);
             rb = (lr - lc * rb) * ib;
             cb = -lc * cb * ib;
             ab = la * ib;
@@ -1582,9 +1636,9 @@ __global__ void __launch_bounds__(32 * P, RS <= 16 ? 2 : 1) k_line_seg(Geo G, Rn
     {
         // separator row: a0 x_{-1} + b0 S_l + c0 x_1 = r0 with x_{-1} the
         // previous segment's last interior row
-        float a0, b0, c0, r0;
+        real a0, b0, c0, r0;
         row(0, a0, b0, c0, r0);
-        float gp = 0.f, vp = 0.f, wp = 0.f;
+        real gp = (real)0, vp = (real)0, wp = (real)0;
         if (l > 0) {
             gp = tail[0][l - 1][lane];
             vp = tail[1][l - 1][lane];
@@ -1599,22 +1653,22 @@ __global__ void __launch_bounds__(32 * P, RS <= 16 ? 2 : 1) k_line_seg(Geo G, Rn
     if (l == 0) {
         // the P separator equations of this lane's line (Thomas); c' and
         // the eliminated rhs replace gamma and rho in place
-        float ib = __fdividef(1.0f, eq[1][0][lane]);
-        float cp = eq[2][0][lane] * ib, rp = eq[3][0][lane] * ib;
+        real ib = rcp_<real>(eq[1][0][lane]);
+        real cp = eq[2][0][lane] * ib, rp = eq[3][0][lane] * ib;
         eq[2][0][lane] = cp;
         eq[3][0][lane] = rp;
 #pragma unroll
         for (int t = 1; t < P; ++t) {
-            const float al = eq[0][t][lane];
-            ib = __fdividef(1.0f, eq[1][t][lane] - al * cp);
+            const real al = eq[0][t][lane];
+            ib = rcp_<real>(eq[1][t][lane] - al * cp);
             cp = eq[2][t][lane] * ib;
             rp = (eq[3][t][lane] - al * rp) * ib;
             eq[2][t][lane] = cp;
             eq[3][t][lane] = rp;
         }
-        float x = rp;
+        real x = rp;
         sep[P - 1][lane] = x;
-        sep[P][lane] = 0.f;
+        sep[P][lane] = (real)0;
 #pragma unroll
         for (int t = P - 2; t >= 0; --t) {
             x = eq[3][t][lane] - eq[2][t][lane] * x;
@@ -1623,22 +1677,22 @@ __global__ void __launch_bounds__(32 * P, RS <= 16 ? 2 : 1) k_line_seg(Geo G, Rn
     }
     __syncthreads();
     if (!live) return;
-    const float Sl = sep[l][lane], Sn = sep[l + 1][lane];
+    const real Sl = sep[l][lane], Sn = sep[l + 1][lane];
     fresh();
 
     // interior rows with both separators known: Thomas with x_0 = S_l and
     // x_RS = S_{l+1}; c' in cq, the eliminated rhs replaces rS
-    float cq[RS];
+    real cq[RS];
     {
-        float la, lb, lc, lr;
+        real la, lb, lc, lr;
         row(1, la, lb, lc, lr);
-        float ib = __fdividef(1.0f, lb);
+        real ib = rcp_<real>(lb);
         cq[1] = lc * ib;
         rS[1] = (lr - la * Sl) * ib;
 #pragma unroll
         for (int e = 2; e < RS; ++e) {
             row(e, la, lb, lc, lr);
-            ib = __fdividef(1.0f, lb - la * cq[e - 1]);
+            ib = rcp_<real>(lb - la * cq[e - 1]);
             cq[e] = lc * ib;
             rS[e] = (lr - la * rS[e - 1]) * ib;
         }
@@ -1650,14 +1704,14 @@ __global__ void __launch_bounds__(32 * P, RS <= 16 ? 2 : 1) k_line_seg(Geo G, Rn
     const bool jlo = AXIS == 0 && VAR == VC && jl == R.js, jhi = AXIS == 0 && VAR == VC && jl == R.je;
     const bool klo = AXIS == 0 && VAR == VC && k == R.ks, khi = AXIS == 0 && VAR == VC && k == R.ke;
     const bool edge = jlo | jhi | klo | khi;
-    auto put = [&](int e, float x) {
+    auto put = [&](int e, real x) {
         if (!FULL && last_seg && e == RS - 1) return;
         const long id = seg + e * st;
         if (AXIS != 0) {
             S[id] = x;
             return;
         }
-        const float v = myq[e * TS] + x;
+        const real v = myq[e * TS] + x;
         A.qn[id] = v;
         if (edge) {
             const long sy = G.sy;
@@ -1675,7 +1729,7 @@ __global__ void __launch_bounds__(32 * P, RS <= 16 ? 2 : 1) k_line_seg(Geo G, Rn
             }
         }
     };
-    float x = Sn;
+    real x = Sn;
 #pragma unroll
     for (int e = RS - 1; e >= 1; --e) {
         x = rS[e] - cq[e] * x;

@@ -26,13 +26,14 @@ def _dp(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
-PRECISIONS = {"fp64": 0, "mixed": 1}
+PRECISIONS = {"fp64": 0, "mixed": 1, "mixed64": 2}
 
 
 class Solver:
     """precision="fp64": the reference's FP64 arithmetic; "mixed": FP32 state
     and stencils, split-TF32 tensor-core DCT, FP64 Poisson mode solve and
-    reductions.  dct_kernel="auto" runs the precision form's DCT passes as
+    reductions; "mixed64": the FP64 form with the WENO5 weights in FP32.
+    dct_kernel="auto" runs the precision form's DCT passes as
     tcgen05 GEMMs where the plane shape allows (ny, nz in {128, 256}; a
     persistent kernel, one CTA per SM), "umma_tile" the same tcgen05 pass
     with one tile per CTA, "mma_sync" the warp-level split-TF32 GEMM.

@@ -4,7 +4,8 @@ form against the plain FP64 step).
     python -m pllcart3d_b200.validate [--workload NAME] [--steps N] [--every K]
                                       [--test FORM] [--ref FORM]
 
-FORM: fp64 (DMMA DCT), fp64-exact (sequential-order DCT), mixed (tcgen05
+FORM: fp64 (the FP64 form), fp64-exact (the reference's operation order,
+sequential-order DCT), mixed64 (FP64 state, FP32 WENO5 weights), mixed (tcgen05
 split-TF32 DCT where the shape allows), mixed-mma (mma.sync split-TF32 DCT),
 mixed-seq (sequential FP32 DCT).  Both runs start from the same seeded
 initial condition and advance in lockstep; every K steps (or at the steps
@@ -38,6 +39,7 @@ VECTORS = {"u_new": ("u_new", "v_new", "w_new"), "v_new": ("u_new", "v_new", "w_
            "v_pg": ("u_pg", "v_pg", "w_pg"), "w_pg": ("u_pg", "v_pg", "w_pg")}
 FORMS = {"fp64": dict(precision="fp64"), "fp64-exact": dict(precision="fp64", exact_dct=True),
          "mixed": dict(precision="mixed"), "mixed-mma": dict(precision="mixed", dct_kernel="mma_sync"),
+         "mixed64": dict(precision="mixed64"),
          "mixed-seq": dict(precision="mixed", exact_dct=True)}
 
 
