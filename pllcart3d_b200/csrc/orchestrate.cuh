@@ -202,13 +202,17 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
     X.alpha = alpha;
     const int lb = tune_line_block(ctx->tune_line);
     bool ydone = false;
+    if constexpr (!std::is_same<real, float>::value && !PLL_FP64_EXACT && VAR == VC) {
+        // FP64 forms: the segmented y solve for concentration (0.65 against
+        // 0.95 ms per step at 512x256x256).  For momentum, whose segments
+        // also stage viscosity rows, one 512-thread block per SM measured
+        // slower than the prefetching sweep (1.12 against 1.00 ms).
+        ydone = launch_line_seg<VAR, 1, real>(ctx, R, X);
+    }
     if constexpr (std::is_same<real, float>::value) {
         // the precision form's partitioned solves: segmented when the line
         // length allows, else for concentration the warp solve of short
-        // lines.  (In FP64 a segment's rows fill a 512-thread block's
-        // registers, one block per SM, and the segmented y solve measured
-        // slower than the prefetching sweep: 1.12 against 1.00 ms per
-        // variable and step at 512x256x256.)
+        // lines
         ydone = launch_line_seg<VAR, 1, real>(ctx, R, X);
         if (!ydone && VAR == VC && nj(R) <= ZP_MAX && nj(R) >= 2 * (ZP_MAX / 32) && !ctx->P.exact_dct) {
             k_adi_y_part<VAR, float><<<dim3((nk(R) + 31) / 32, ni(R)), 256, adi_y_part_smem<float>(), ctx->st>>>(
@@ -954,6 +958,7 @@ bool alloc_state(pllgpu_ctx* c)
         cudaFuncSetAttribute(k_adi_y_part<VW, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)adi_y_part_smem<float>());
     }
+    if constexpr (!std::is_same<real, float>::value && !PLL_FP64_EXACT) line_seg_attrs<VC, real>();
     if constexpr (std::is_same<real, float>::value) {
         line_seg_attrs<VC, real>();
         line_seg_attrs<VU, real>();
