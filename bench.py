@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--precision", default="all", choices=["all", "both", "fp64", "mixed", "mixed64"],
                     help="forms to time (all: fp64, mixed64, mixed; both: fp64, mixed); the headline value is "
                          "--headline's")
+    ap.add_argument("--explicit-kernel", default="auto", choices=["auto", "direct", "tma"],
+                    help="explicit-operator kernel of every timed form (Solver's explicit_kernel)")
     ap.add_argument("--headline", default="mixed64", choices=["fp64", "mixed", "mixed64"],
                     help="the form whose throughput is `value`: mixed64 is the form that meets the 1e-5 c "
                          "accuracy target of the metric")
@@ -230,7 +232,7 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
-def measure(prm, ic, form, steps, warmup, ws, local, profile_steps=2):
+def measure(prm, ic, form, steps, warmup, ws, local, profile_steps=2, explicit_kernel="auto"):
     """Device-timed steps of one precision form + per-kernel event profile."""
     import ctypes
 
@@ -238,7 +240,7 @@ def measure(prm, ic, form, steps, warmup, ws, local, profile_steps=2):
 
     from pllcart3d_b200.solver import Solver
 
-    s = Solver(prm, device=local, exact_dct=False, use_graph=True, precision=form)
+    s = Solver(prm, device=local, exact_dct=False, use_graph=True, precision=form, explicit_kernel=explicit_kernel)
     s.load_ic(ic)
     stream = torch.cuda.ExternalStream(s._L.pllgpu_stream(s._h), device=local)
     s.step(warmup)
@@ -397,7 +399,7 @@ def run_ours(args, ws, rank, local):
     forms = {}
     chosen = {"all": ("fp64", "mixed64", "mixed"), "both": ("fp64", "mixed")}.get(args.precision, (args.precision,))
     for form in chosen:
-        m = measure(prm, ic, form, args.steps, args.warmup, ws, local)
+        m = measure(prm, ic, form, args.steps, args.warmup, ws, local, explicit_kernel=args.explicit_kernel)
         prec = "fp32" if form == "mixed" else "fp64"
         sb = roofline.step_bytes(cells, prec)
         m["value"] = replica_value(cells, args.steps, ws, m["ms"])

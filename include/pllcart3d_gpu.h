@@ -72,7 +72,12 @@ typedef struct pllgpu_params {
                               GEMMs (persistent, one CTA per SM) where ny, nz
                               are 128 or 256, else mma.sync; 1 = mma.sync
                               split-TF32 always; 2 = tcgen05, one tile per CTA */
-    int reserved[4];
+    int explicit_kernel;   /* explicit operator, exact_dct 0: 0 = default (FP64
+                              forms: TMA-staged plane-marching kernel; the
+                              precision form: cell pairs in FP32x2), 1 = the
+                              per-cell kernel (FP64) / cell pairs (FP32), 2 =
+                              the TMA-staged kernel in either form           */
+    int reserved[3];
 } pllgpu_params;
 
 typedef struct pllgpu_ctx pllgpu_ctx;

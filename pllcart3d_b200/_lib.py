@@ -52,7 +52,7 @@ class Params(ctypes.Structure):
         ("Re", _D), ("Pe", _D), ("Vratio", _D), ("Fx", _D), ("Fy", _D),
         ("CFLmax", _D), ("Timestep", _D), ("Mum", _D), ("Lambda", _D),
         ("precision", _I), ("exact_dct", _I), ("use_graph", _I),
-        ("dct_kernel", _I), ("reserved", _I * 4),
+        ("dct_kernel", _I), ("explicit_kernel", _I), ("reserved", _I * 3),
     ]
 
 

@@ -100,13 +100,17 @@ void launch_explicit(pllgpu_ctx* ctx, const real* un, const real* vn, const real
     int bx, by;
     tune_exp_block(ctx->tune_exp, bx, by);
     if constexpr (std::is_same<real, float>::value) {
+        if (ctx->P.explicit_kernel == 2 && !ctx->P.exact_dct && launch_explicit_tma<real, VAR>(ctx, A)) {
+            mark(ctx, lab[VAR]);
+            return;
+        }
         // cell pairs (k, k + EP_DK): blocks of EP_DK x rows, the same threads
         // per block as the tuned shape
         const dim3 blk(EP_DK, bx * by / EP_DK);
         const dim3 grid((nk(R) + 2 * EP_DK - 1) / (2 * EP_DK), (nj(R) + blk.y - 1) / blk.y, ni(R));
         k_explicit2<VAR><<<grid, blk, 0, ctx->st>>>(ctx->G, R, ctx->K, A);
     } else {
-        if (!ctx->xt_on || !launch_explicit_tma<real, VAR>(ctx, A)) {
+        if (!ctx->xt_on || ctx->P.explicit_kernel == 1 || !launch_explicit_tma<real, VAR>(ctx, A)) {
             const dim3 blk(bx, by);
             k_explicit<VAR, real><<<box_grid(nk(R), nj(R), ni(R), blk), blk, 0, ctx->st>>>(ctx->G, R, ctx->K, A);
         }
@@ -974,6 +978,16 @@ bool alloc_state(pllgpu_ctx* c)
     cudaFuncSetAttribute(k_adi_z_tiled<VW, real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)adi_z_smem_bytes<VW, real>());
     if constexpr (std::is_same<real, float>::value) {
+        if (p->explicit_kernel == 2) {
+            cudaFuncSetAttribute(k_explicit_tma<VC, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 XtSmem<float, VC>::DYN);
+            cudaFuncSetAttribute(k_explicit_tma<VU, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 XtSmem<float, VU>::DYN);
+            cudaFuncSetAttribute(k_explicit_tma<VV, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 XtSmem<float, VV>::DYN);
+            cudaFuncSetAttribute(k_explicit_tma<VW, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 XtSmem<float, VW>::DYN);
+        }
         const bool shape_ok = (p->ny == 128 || p->ny == 256) && (p->nz == 128 || p->nz == 256);
         if (shape_ok && !p->exact_dct && p->dct_kernel != 1 && !setup_umma(c)) return false;
     } else {

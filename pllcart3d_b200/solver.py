@@ -37,14 +37,19 @@ class Solver:
     tcgen05 GEMMs where the plane shape allows (ny, nz in {128, 256}; a
     persistent kernel, one CTA per SM), "umma_tile" the same tcgen05 pass
     with one tile per CTA, "mma_sync" the warp-level split-TF32 GEMM.
+    explicit_kernel="auto" runs the explicit operator as the TMA-staged
+    plane-marching kernel in the FP64 forms and on FP32x2 cell pairs in the
+    precision form; "direct" the per-cell (FP64) / paired (FP32) kernel,
+    "tma" the TMA-staged kernel in either form.
     exact_dct=True sums the DCTs in sequential order and, in the precision
     form, runs every line and mode solve as the sequential Thomas sweep (the
     default: the partitioned line solves and, with the tcgen05 DCT, the
     FP32-scratch mode solve)."""
 
     def __init__(self, params: Params, device: int = 0, exact_dct: bool = False,
-                 use_graph: bool = True, precision: str = "fp64", dct_kernel: str = "auto"):
-        p = self.c_params(params, exact_dct, use_graph, precision, dct_kernel)
+                 use_graph: bool = True, precision: str = "fp64", dct_kernel: str = "auto",
+                 explicit_kernel: str = "auto"):
+        p = self.c_params(params, exact_dct, use_graph, precision, dct_kernel, explicit_kernel)
         self.params = params
         self.precision = precision
         self._L = _lib.lib()
@@ -64,7 +69,7 @@ class Solver:
 
     @staticmethod
     def c_params(params: Params, exact_dct: bool = False, use_graph: bool = True,
-                 precision: str = "fp64", dct_kernel: str = "auto"):
+                 precision: str = "fp64", dct_kernel: str = "auto", explicit_kernel: str = "auto"):
         """The pllgpu_params struct of a run."""
         params.validate()
         p = _lib.Params()
@@ -79,6 +84,7 @@ class Solver:
         p.exact_dct = int(bool(exact_dct))
         p.use_graph = int(bool(use_graph))
         p.dct_kernel = {"auto": 0, "mma_sync": 1, "umma_tile": 2}[dct_kernel]
+        p.explicit_kernel = {"auto": 0, "direct": 1, "tma": 2}[explicit_kernel]
         return p
 
     # ---- lifetime ---------------------------------------------------------

@@ -168,3 +168,22 @@ def test_mixed64_tracks_the_fp64_form():
     assert rel_maxnorm(b.get("c_new"), a.get("c_new")) <= 1e-6
     for f in ("u_new", "v_new", "w_new"):
         assert rel_vector(b.get, a.get, f) <= 1e-5, f
+
+
+def test_tma_explicit_kernel_in_the_precision_form():
+    """The TMA-staged plane-marching explicit operator (selectable in the
+    precision form, the default of the FP64 forms) computes each cell with
+    the per-cell FP32 arithmetic; one step agrees with the paired kernel's to
+    FP32 rounding."""
+    from pllcart3d_b200.solver import Solver
+
+    wl = workload("fingering-64x64x64")
+    ic = workload_fields(wl)
+    a = Solver(wl.params, precision="mixed")
+    b = Solver(wl.params, precision="mixed", explicit_kernel="tma")
+    for s in (a, b):
+        s.load_ic(ic)
+        s.step(1)
+        assert s.status() == 0
+    for f in ("c_new", "u_new", "v_new", "w_new"):
+        assert rel_vector(b.get, a.get, f) <= 1e-5, f
