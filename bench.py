@@ -273,14 +273,16 @@ def measure(prm, ic, form, steps, warmup, ws, local, profile_steps=2, explicit_k
     return out
 
 
+# dense GEMM peaks of the DCT kernels' own arithmetic, measured on this
+# pool's B200s with `python -m pllcart3d_b200.peaks` (cuBLAS, 8192^3, burst)
+TF32_TFLOPS = 730.2
+FP64_TFLOPS = 35.5
+
+
 def tensor_peak():
-    """Dense TF32 tensor peak: half the measured BF16 GEMM rate (B200 runs
-    TF32 at half the BF16 rate); None without a measurement."""
-    try:
-        with open(PEAKS) as f:
-            return float(json.load(f)["bf16_tflops"]) / 2.0
-    except Exception:
-        return None
+    """Dense TF32 tensor peak the split-TF32 DCT passes are measured
+    against (the measured burst rate)."""
+    return TF32_TFLOPS
 
 
 # DRAM traffic over algorithmic bytes of a launch, from the ncu captures of
