@@ -128,7 +128,8 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--members", type=int, default=64)
     ap.add_argument("--steps", type=int, default=500)
-    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed64", "mixed"])
+    ap.add_argument("--out", default=None, help="also write the report JSON to this file")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--snapshots", default=None)
     ap.add_argument("--every", type=int, default=8)
@@ -183,14 +184,18 @@ def main(argv=None) -> int:
             p = w.params
             np.savez(os.path.join(args.snapshots, f"member{i:03d}.npz"), states=np.stack(snaps[i]),
                      R=-p.Vratio, Pe=p.Pe, Re=p.Re, every=args.every)
-    print(json.dumps({
+    rep = {
         "workload": f"ensemble of {len(wls)} runs",
         "precision": args.precision, "steps": done, "timed_steps": timed,
         "cells": ens.cells(), "ensemble_cell_steps_per_s": ens_cells,
         "sequential_cell_steps_per_s": seq_cells, "speedup": ens_cells / seq_cells,
         "launches_per_graph_step": ens.launches_per_step, "autotune_steps": tuned_steps,
         "members_equal_to_single_runs": mismatches == 0,
-        "grids": [list(w.params.shape) for w in wls]}))
+        "grids": [list(w.params.shape) for w in wls]}
+    print(json.dumps(rep))
+    if args.out:
+        with open(args.out, "w") as f:
+            json.dump(rep, f, indent=1)
     ens.close()
     return 0 if mismatches == 0 else 1
 

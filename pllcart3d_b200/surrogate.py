@@ -414,8 +414,12 @@ class Surrogate:
         self.next = torch.empty_like(self.cells)
         self.x16 = torch.empty((self.V, 16), dtype=torch.bfloat16, device="cuda")
 
-    def advance(self, solver, R, Pe):
-        """One window: network prediction, then the solver's projection."""
+    def advance(self, solver, R, Pe, mass_target=None, dV=None):
+        """One window: network prediction, then the solver's projection.
+        With `mass_target` (and the cell volume dV) the predicted c is made
+        to carry that mass: the difference is spread evenly over the cells
+        of the mixing zone (0.01 < c < 0.99), leaving the pure-fluid regions
+        as predicted."""
         import torch
 
         L, st = nnlib(), _stream()
@@ -425,6 +429,13 @@ class Surrogate:
         _ok(L.pllnn_pack_input(_p(self.cells), self.V, r, p, _p(self.norm_t), _p(self.x16), st), "pack input")
         out = self.net.forward(self.x16, (1,) + self.grid)
         _ok(L.pllnn_apply_delta(_p(self.cells), _p(out), self.V, _p(self.dscale_t), _p(self.next), st), "apply")
+        if mass_target is not None:
+            c = self.next[:, 3]   # cells are (u, v, w, c)
+            zone = (c > 0.01) & (c < 0.99)
+            n = int(zone.sum().item())
+            if n > 0:
+                m = float(c.double().sum().item()) * dV
+                c[zone] += float((mass_target - m) / (n * dV))
         torch.cuda.synchronize()
         solver.unpack_cells(self.next.data_ptr())
         solver.project()
@@ -434,7 +445,7 @@ def rel(a, b):
     return abs(a - b) / max(abs(b), 1e-30)
 
 
-def rollout(sur: Surrogate, wl, steps=2000, judge_every=4, tol=1e-3, precision="fp64"):
+def rollout(sur: Surrogate, wl, steps=2000, judge_every=4, tol=1e-3, precision="fp64", mass_fix=True):
     """Surrogate + judge rollout of `steps` steps; returns a report.
 
     Windows of 8 steps.  Every `judge_every`-th window the plain solver runs
@@ -443,7 +454,12 @@ def rollout(sur: Surrogate, wl, steps=2000, judge_every=4, tol=1e-3, precision="
     (or the solver cannot step from that start).  A rejection, or a
     non-finite prediction anywhere, sends the rollout back to the last state
     a judge verified, and the solver runs every window since: the state is
-    verified at every judged window."""
+    verified at every judged window.
+
+    mass_fix: the network's c is corrected to the mass the run had at the
+    window's start plus the mass change of the previous window (the inflow
+    adds mass at a nearly constant rate); the judge's own result is never
+    used for it."""
     import torch
 
     from . import _lib
@@ -483,12 +499,17 @@ def rollout(sur: Surrogate, wl, steps=2000, judge_every=4, tol=1e-3, precision="
         Sgood.copy_state_from(S)
         wgood = w + 1
 
+    dV = wl.params.dx * wl.params.dy * wl.params.dz
+    m_prev = None   # mass at the previous window's start
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for w in range(nwin):
         judge = (w % judge_every) == judge_every - 1
         judged_ok = solver_window(S) if judge else False
-        sur.advance(S, R, Pe)
+        m_now = S.diagnostics()["mass"] if mass_fix else None
+        target = (2.0 * m_now - m_prev) if (mass_fix and m_prev is not None) else None
+        sur.advance(S, R, Pe, target, dV)
+        m_prev = m_now
         ds = S.diagnostics()
         finite = all(math.isfinite(x) for x in ds.values())
         if not finite:
@@ -548,10 +569,14 @@ def main(argv=None) -> int:
     ap.add_argument("--grid", default="128x64x64")
     ap.add_argument("--save", default=None)
     ap.add_argument("--load", default=None, help="a network saved by --save: skip training")
+    ap.add_argument("--data-precision", default="fp64", choices=["fp64", "mixed64", "mixed"],
+                    help="form of the runs that make the training data (the judge runs the FP64 form)")
+    ap.add_argument("--no-mass-fix", action="store_true")
+    ap.add_argument("--out", default=None, help="also write the report JSON to this file")
     args = ap.parse_args(argv)
     grid = tuple(int(t) for t in args.grid.split("x"))
     t0 = time.perf_counter()
-    ds, wls = generate_data(args.runs, grid, args.data_steps)
+    ds, wls = generate_data(args.runs, grid, args.data_steps, precision=args.data_precision)
     t_data = time.perf_counter() - t0
     # hold out the last run for evaluation and the rollout
     per_run = len(ds.a) // args.runs
@@ -586,12 +611,17 @@ def main(argv=None) -> int:
     print(json.dumps({"phase": "trained", "train_s": t_train, "heldout_mse": loss,
                       "heldout_mse_persistence": loss0, "loss_curve": curve}), flush=True)
     sur = Surrogate(net, tr.norm, tr.dscale, grid)
-    rep = rollout(sur, wls[-1], args.rollout)
+    rep = rollout(sur, wls[-1], args.rollout, mass_fix=not args.no_mass_fix)
     rep.update({"grid": list(grid), "params": net.n_params(), "train_steps": args.train_steps,
+                "data_precision": args.data_precision, "mass_fix": not args.no_mass_fix, "runs": args.runs,
+                "data_steps": args.data_steps,
                 "batch": args.batch, "train_s": t_train, "train_ms_per_step": 1e3 * t_train / max(1, args.train_steps),
                 "data_s": t_data, "samples": len(ds.a), "heldout_mse": loss, "heldout_mse_persistence": loss0,
                 "loss_curve": curve})
     print(json.dumps(rep))
+    if args.out:
+        with open(args.out, "w") as f:
+            json.dump(rep, f, indent=1)
     return 0
 
 
