@@ -5,7 +5,7 @@
   multiply-add is contracted (the reference's own arithmetic has none), the
   FP64 form and the precision form's FP32 kernels with contraction;
 * ``libpllnn.so``            - the learned surrogate's BF16 tensor-core kernels
-  (convolution forward / backward, pooling, upsampling, Adam);
+  (tcgen05 and mma.sync convolutions, pooling, upsampling, Adam);
 * ``libpllcart3d_dropin.so`` - the reference-signature drop-in layer (plain C,
   compiled with gcc because the reference's structures name a member ``new``).
 
@@ -77,7 +77,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         for o in objs:
             os.remove(o)
     nsrc = os.path.join(CSRC, "nn.cu")
-    if os.path.exists(nsrc) and (force or _stale(NNLIB, [nsrc, __file__])):
+    if os.path.exists(nsrc) and (force or _stale(NNLIB, [nsrc, os.path.join(CSRC, "nn_umma.cuh"), __file__])):
         cmd = [_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas",
                "-warn-spills", "-shared", "-cudart", "static", nsrc, "-o", NNLIB]
         if verbose:

@@ -3,6 +3,11 @@
 // and Adam, hand-written for the BF16 tensor cores (mma.sync m16n8k16, BF16
 // operands, FP32 accumulation).
 //
+// The forward convolution (and so the input gradient) runs on the 5th-
+// generation tensor cores where the shapes allow (nn_umma.cuh: tcgen05.mma
+// with a TMEM accumulator, TMA-staged operands whose out-of-bounds fill is
+// the zero padding), else on the mma.sync kernel below.
+//
 // Layout: activations are channels-last [n][d][h][w][c] (voxel-major, c
 // contiguous), BF16 as operands of the convolutions, FP32 for
 // pre-activations and gradients that are accumulated.  Weights are
@@ -20,10 +25,14 @@
 //    over voxel chunks, FP32 atomics into the gradient;
 //  * 2x average pooling, 2x nearest upsampling, channel concatenation,
 //    activation backward with the bias-gradient reduction, MSE loss, Adam.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
+
+#include "nn_umma.cuh"
 
 typedef __nv_bfloat16 bf16;
 
@@ -516,6 +525,112 @@ __global__ void k_apply_delta(const float* __restrict__ a, const float* __restri
 
 inline unsigned nblk(long n, int b) { return (unsigned)((n + b - 1) / b); }
 
+// ---- the tcgen05 convolution: tensor maps, shape checks, dispatch ----------
+int g_conv_path = 0;   // 0: tcgen05 where the shapes allow, 1: mma.sync, 2: tcgen05 or fail
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn nn_encode()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// the geometry of the tcgen05 path, false when the shapes do not fit it:
+// tiles of 128 voxels made of whole w rows (W divides 128), hb rows of h and
+// db slices of d; Cout a multiple of the column tile; Cin a multiple of 16
+bool cu_geom(int N, int D, int H, int W, int Cin, int Cout, int ksize, CuGeom& g, int& BN, int& CK)
+{
+    const long V = (long)N * D * H * W;
+    if (V % CU_BM || W > CU_BM || CU_BM % W || Cin % 16 || Cout % 16) return false;
+    const int hb = (CU_BM / W) < H ? (CU_BM / W) : H;
+    if (H % hb || (CU_BM / W) % hb) return false;
+    const int db = CU_BM / (W * hb);
+    if (db > D || D % db) return false;
+    BN = Cout >= 128 ? 128 : Cout >= 64 ? 64 : Cout >= 32 ? 32 : 16;
+    if (Cout % BN) return false;
+    CK = Cin % 64 == 0 ? 64 : Cin % 32 == 0 ? 32 : 16;
+    g = CuGeom{N, D, H, W, hb, db, Cin, Cout, ksize};
+    return true;
+}
+
+bool cu_maps(const CuGeom& g, int BN, int CK, const void* X, const void* Wt, CUtensorMap* mx, CUtensorMap* mw)
+{
+    EncodeTiledFn fn = nn_encode();
+    if (!fn) return false;
+    const CUtensorMapSwizzle sw = CK == 64 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                : CK == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
+    const cuuint64_t c2 = (cuuint64_t)g.Cin * 2;
+    const cuuint64_t xd[5] = {(cuuint64_t)g.Cin, (cuuint64_t)g.W, (cuuint64_t)g.H, (cuuint64_t)g.D, (cuuint64_t)g.N};
+    const cuuint64_t xs[4] = {c2, c2 * g.W, c2 * g.W * g.H, c2 * g.W * g.H * g.D};
+    const cuuint32_t xb[5] = {(cuuint32_t)CK, (cuuint32_t)g.W, (cuuint32_t)g.hb, (cuuint32_t)g.db, 1};
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    if (fn(mx, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)X, xd, xs, xb, es, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    const int taps = g.ksize * g.ksize * g.ksize;
+    const cuuint64_t wd[3] = {(cuuint64_t)g.Cin, (cuuint64_t)taps, (cuuint64_t)g.Cout};
+    const cuuint64_t ws[2] = {c2, c2 * taps};
+    const cuuint32_t wb[3] = {(cuuint32_t)CK, 1, (cuuint32_t)BN};
+    return fn(mw, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void*)Wt, wd, ws, wb, es, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int BN, int CK>
+bool cu_launch(const CUtensorMap& mx, const CUtensorMap& mw, const CuGeom& g, const float* bias, float* Y32,
+               void* Y16, int act, float slope, cudaStream_t st)
+{
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_conv_umma<BN, CK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)CuSmem<BN, CK>::DYN) != cudaSuccess)
+            return false;
+        attr = true;
+    }
+    const long V = (long)g.N * g.D * g.H * g.W;
+    const dim3 grid((unsigned)(V / CU_BM), (unsigned)(g.Cout / BN));
+    k_conv_umma<BN, CK><<<grid, CU_THREADS, CuSmem<BN, CK>::DYN, st>>>(mx, mw, g, bias, Y32, (__nv_bfloat16*)Y16,
+                                                                         act, slope);
+    return true;
+}
+
+template <int BN>
+bool cu_launch_ck(int CK, const CUtensorMap& mx, const CUtensorMap& mw, const CuGeom& g, const float* bias,
+                  float* Y32, void* Y16, int act, float slope, cudaStream_t st)
+{
+    if (CK == 64) return cu_launch<BN, 64>(mx, mw, g, bias, Y32, Y16, act, slope, st);
+    if (CK == 32) return cu_launch<BN, 32>(mx, mw, g, bias, Y32, Y16, act, slope, st);
+    return cu_launch<BN, 16>(mx, mw, g, bias, Y32, Y16, act, slope, st);
+}
+
+// the forward convolution on tcgen05; false when the shapes or the tensor
+// maps do not fit (the caller then runs the mma.sync kernel)
+bool conv_umma(const void* X, int N, int D, int H, int W, int Cin, const void* Wt, const float* bias, int Cout,
+               int ksize, float* Y32, void* Y16, int act, float slope, cudaStream_t st)
+{
+    CuGeom g;
+    int BN = 0, CK = 0;
+    if (!cu_geom(N, D, H, W, Cin, Cout, ksize, g, BN, CK)) return false;
+    if (((uintptr_t)Y32 & 15) || ((uintptr_t)Y16 & 15) || ((uintptr_t)bias & 3)) return false;
+    CUtensorMap mx, mw;
+    std::memset(&mx, 0, sizeof(mx));
+    std::memset(&mw, 0, sizeof(mw));
+    if (!cu_maps(g, BN, CK, X, Wt, &mx, &mw)) return false;
+    if (BN == 128) return cu_launch_ck<128>(CK, mx, mw, g, bias, Y32, Y16, act, slope, st);
+    if (BN == 64) return cu_launch_ck<64>(CK, mx, mw, g, bias, Y32, Y16, act, slope, st);
+    if (BN == 32) return cu_launch_ck<32>(CK, mx, mw, g, bias, Y32, Y16, act, slope, st);
+    return cu_launch_ck<16>(CK, mx, mw, g, bias, Y32, Y16, act, slope, st);
+}
+
 }  // namespace
 
 extern "C" {
@@ -528,6 +643,9 @@ int pllnn_conv_fwd(const void* X, int N, int D, int H, int W, int Cin, const voi
     const Vol g{N, D, H, W};
     const long V = (long)N * D * H * W;
     cudaStream_t st = (cudaStream_t)stream;
+    if (g_conv_path != 1 && conv_umma(X, N, D, H, W, Cin, Wt, bias, Cout, ksize, Y32, Y16, act, slope, st))
+        return cudaGetLastError() == cudaSuccess ? 0 : 2;
+    if (g_conv_path == 2) return 6;
     if (Cout <= 32) {
         dim3 grid(nblk(V, CBM), nblk(Cout, 32));
         k_conv_fwd<32><<<grid, 256, 0, st>>>((const bf16*)X, g, Cin, (const bf16*)Wt, bias, Cout, ksize, Y32,
@@ -538,6 +656,26 @@ int pllnn_conv_fwd(const void* X, int N, int D, int H, int W, int Cin, const voi
                                              (bf16*)Y16, act, slope);
     }
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// which kernel the forward convolution uses: 0 the tcgen05 kernel where the
+// shapes allow (default), 1 the mma.sync kernel, 2 the tcgen05 kernel or
+// status 6; returns the previous setting
+int pllnn_set_conv_path(int path)
+{
+    const int old = g_conv_path;
+    if (path >= 0 && path <= 2) g_conv_path = path;
+    return old;
+}
+
+// the library's status bits (0x100: a bounded wait of the tcgen05
+// convolution ran out), cleared by the read
+int pllnn_status(void)
+{
+    int v = 0, z = 0;
+    if (cudaMemcpyFromSymbol(&v, g_nn_status, sizeof(int)) != cudaSuccess) return -1;
+    if (v) cudaMemcpyToSymbol(g_nn_status, &z, sizeof(int));
+    return v;
 }
 
 int pllnn_conv_wgrad(const void* G, const void* X, int N, int D, int H, int W, int Cin, int Cout, int ksize,

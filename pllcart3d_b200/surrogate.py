@@ -73,6 +73,8 @@ def nnlib():
         L.pllnn_pack_input.argtypes = [P, Lg, F, F, P, P, P]
         L.pllnn_pack_target.argtypes = [P, P, Lg, P, P, P]
         L.pllnn_apply_delta.argtypes = [P, P, Lg, P, P, P]
+        L.pllnn_set_conv_path.argtypes = [I]
+        L.pllnn_status.argtypes = []
         _nn = L
     return _nn
 
@@ -399,6 +401,9 @@ class Trainer:
 
 # ---- rollout ---------------------------------------------------------------
 
+MASS_FIX_MIN_ZONE = 0.005   # the mixing zone's share of the cells below which c is left as predicted
+MASS_FIX_MAX_SHIFT = 0.02   # largest change of c per zone cell the mass correction applies
+
 class Surrogate:
     """Network + normalisation of one grid, acting on a Solver's state."""
 
@@ -419,7 +424,8 @@ class Surrogate:
         With `mass_target` (and the cell volume dV) the predicted c is made
         to carry that mass: the difference is spread evenly over the cells
         of the mixing zone (0.01 < c < 0.99), leaving the pure-fluid regions
-        as predicted."""
+        as predicted; skipped when the zone is under MASS_FIX_MIN_ZONE of the
+        cells or the shift would exceed MASS_FIX_MAX_SHIFT."""
         import torch
 
         L, st = nnlib(), _stream()
@@ -433,9 +439,14 @@ class Surrogate:
             c = self.next[:, 3]   # cells are (u, v, w, c)
             zone = (c > 0.01) & (c < 0.99)
             n = int(zone.sum().item())
-            if n > 0:
+            # only while the mixing zone is a real part of the volume and the
+            # shift stays small: once the displaced fluid has left the box
+            # the zone is a few cells and the mass history no longer a guide
+            if n >= MASS_FIX_MIN_ZONE * self.V:
                 m = float(c.double().sum().item()) * dV
-                c[zone] += float((mass_target - m) / (n * dV))
+                shift = (mass_target - m) / (n * dV)
+                if abs(shift) <= MASS_FIX_MAX_SHIFT:
+                    c[zone] += float(shift)
         torch.cuda.synchronize()
         solver.unpack_cells(self.next.data_ptr())
         solver.project()
@@ -556,6 +567,51 @@ def rollout(sur: Surrogate, wl, steps=2000, judge_every=4, tol=1e-3, precision="
             "wall_s_rollout": t_roll, "wall_s_plain": t_plain, "speedup": t_plain / t_roll}
 
 
+def bench_conv(batch=8, grid=(128, 64, 64), reps=10):
+    """Forward convolution of every U-Net layer at its own level, on the
+    tcgen05 kernel and on the mma.sync kernel: mean ms per launch (CUDA
+    events) and TFLOP/s (2 x voxels x taps x Cin x Cout per launch)."""
+    import torch
+
+    L, st = nnlib(), _stream()
+    rng = np.random.default_rng(0)
+    levels = {"e1": 0, "e2": 1, "e3": 2, "e4": 3, "d3": 2, "d2": 1, "d1": 0, "out": 0}
+    rows = []
+    for n, ci, co, k, a in LAYERS:
+        s_ = levels[n]
+        vol = (batch, grid[0] >> s_, grid[1] >> s_, grid[2] >> s_)
+        V = int(np.prod(vol))
+        x = torch.tensor(rng.standard_normal((V, ci)), dtype=torch.bfloat16, device="cuda")
+        w = torch.tensor(rng.standard_normal((co, k ** 3, ci)) * 0.05, dtype=torch.bfloat16, device="cuda")
+        b = torch.zeros(co, dtype=torch.float32, device="cuda")
+        z = torch.empty((V, co), dtype=torch.float32, device="cuda")
+        y = torch.empty((V, co), dtype=torch.bfloat16, device="cuda")
+        flops = 2.0 * V * k ** 3 * ci * co
+        row = {"layer": n, "vol": list(vol), "cin": ci, "cout": co, "k": k}
+        for path, name in ((2, "tcgen05"), (1, "mma_sync")):
+            L.pllnn_set_conv_path(path)
+            code = L.pllnn_conv_fwd(_p(x), *vol, ci, _p(w), _p(b), co, k, _p(z), _p(y), a, SLOPE, st)
+            if code:
+                row[name] = None
+                continue
+            torch.cuda.synchronize()
+            e0, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                L.pllnn_conv_fwd(_p(x), *vol, ci, _p(w), _p(b), co, k, _p(z), _p(y), a, SLOPE, st)
+            e1_.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1_) / reps
+            row[name] = {"ms": ms, "tflops": flops / (ms / 1e3) / 1e12}
+        L.pllnn_set_conv_path(0)
+        rows.append(row)
+    tot = {name: sum(r[name]["ms"] for r in rows if r.get(name)) for name in ("tcgen05", "mma_sync")}
+    fl = sum(2.0 * np.prod(r["vol"]) * r["k"] ** 3 * r["cin"] * r["cout"] for r in rows)
+    return {"batch": batch, "grid": list(grid), "layers": rows,
+            "forward_ms": tot, "forward_tflops": {k_: fl / (v / 1e3) / 1e12 for k_, v in tot.items()},
+            "status": L.pllnn_status()}
+
+
 def main(argv=None) -> int:
     import torch
 
@@ -573,8 +629,17 @@ def main(argv=None) -> int:
                     help="form of the runs that make the training data (the judge runs the FP64 form)")
     ap.add_argument("--no-mass-fix", action="store_true")
     ap.add_argument("--out", default=None, help="also write the report JSON to this file")
+    ap.add_argument("--bench-conv", action="store_true",
+                    help="only time every layer's forward convolution on both kernels")
     args = ap.parse_args(argv)
     grid = tuple(int(t) for t in args.grid.split("x"))
+    if args.bench_conv:
+        rep = bench_conv(args.batch, grid)
+        print(json.dumps(rep))
+        if args.out:
+            with open(args.out, "w") as f:
+                json.dump(rep, f, indent=1)
+        return 0
     t0 = time.perf_counter()
     ds, wls = generate_data(args.runs, grid, args.data_steps, precision=args.data_precision)
     t_data = time.perf_counter() - t0

@@ -148,3 +148,43 @@ def test_training_beats_persistence():
     after, persist2 = tr.eval_loss(held)
     assert persist == pytest.approx(persist2, rel=1e-5)   # FP32 atomics: order varies
     assert after < 0.5 * persist, (before, after, persist)
+
+
+@pytest.mark.parametrize("k,ci,co,vol", [
+    (3, 16, 32, (1, 8, 16, 64)),    # the first encoder level: 128-voxel tiles of two w rows
+    (3, 64, 64, (1, 8, 32, 32)),
+    (3, 384, 128, (2, 8, 16, 16)),  # a decoder level (concatenated channels)
+    (3, 128, 256, (1, 16, 8, 8)),   # tiles spanning two d slices; two column tiles
+    (3, 96, 32, (1, 4, 16, 64)),
+    (1, 32, 16, (1, 8, 16, 64)),    # the 1x1x1 output convolution
+])
+def test_tcgen05_conv_matches_mma_sync(k, ci, co, vol):
+    """The tcgen05 convolution (TMA-staged operands, zero padding from the
+    TMA out-of-bounds fill, TMEM accumulator) against the mma.sync kernel on
+    the same BF16 inputs: FP32 sums of the same products in another order."""
+    import torch
+
+    from pllcart3d_b200 import surrogate as S
+
+    L = S.nnlib()
+    rng = np.random.default_rng(ci * 7 + co)
+    x = _t(_bf16(rng.standard_normal(vol + (ci,))).reshape(-1, ci), torch.bfloat16)
+    w = _t(_bf16(rng.standard_normal((co, k ** 3, ci)) / np.sqrt(k ** 3 * ci)), torch.bfloat16)
+    b = _t(rng.standard_normal(co), torch.float32)
+    V = int(np.prod(vol))
+    outs = []
+    try:
+        for path in (1, 2):
+            L.pllnn_set_conv_path(path)
+            z = torch.full((V, co), float("nan"), dtype=torch.float32, device="cuda")
+            y = torch.empty((V, co), dtype=torch.bfloat16, device="cuda")
+            assert L.pllnn_conv_fwd(S._p(x), *vol, ci, S._p(w), S._p(b), co, k, S._p(z), S._p(y), 1, S.SLOPE,
+                                    S._stream()) == 0
+            torch.cuda.synchronize()
+            outs.append((z.cpu().numpy(), y.float().cpu().numpy()))
+    finally:
+        L.pllnn_set_conv_path(0)
+    assert L.pllnn_status() == 0
+    assert np.isfinite(outs[1][0]).all()
+    assert _relerr(outs[1][0], outs[0][0]) < 1e-5
+    assert _relerr(outs[1][1], outs[0][1]) < 1e-2
