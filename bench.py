@@ -288,15 +288,15 @@ def tensor_peak():
 # DRAM traffic over algorithmic bytes of a launch, from the ncu captures of
 # the 256x128x128 case (profiles/); traffic grows with the cells processed,
 # so a full launch's traffic is this ratio times its algorithmic bytes
-TRAFFIC_RATIO = {("k_explicit2", "fp32"): 1.05, ("k_explicit", "fp64"): 1.04}
+TRAFFIC_RATIO = {("k_explicit2", "fp32"): 1.05, ("k_explicit", "fp64"): 1.04, ("k_explicit_tma", "fp64"): 1.04}
 
 
-def roofline_of(kernels, nprof, cells, precision, dims=None):
+def roofline_of(kernels, nprof, cells, precision, dims=None, form=None, explicit="auto"):
     """Roofline of the kernel family with the largest share of the step."""
     hbm, peak_kind = peaks()
     fam = {}
     for lab, v in kernels.items():
-        f = roofline.family(lab, precision)
+        f = roofline.family(lab, precision, form, explicit)
         if f is None:
             continue
         d = fam.setdefault(f, {"ms": 0.0, "launches": 0, "bytes": 0.0, "labels": []})
@@ -405,7 +405,8 @@ def run_ours(args, ws, rank, local):
         prec = "fp32" if form == "mixed" else "fp64"
         sb = roofline.step_bytes(cells, prec)
         m["value"] = replica_value(cells, args.steps, ws, m["ms"])
-        m["roofline"] = roofline_of(m["kernels"], m["profile_steps"], cells, prec, (prm.nx, prm.ny, prm.nz))
+        m["roofline"] = roofline_of(m["kernels"], m["profile_steps"], cells, prec, (prm.nx, prm.ny, prm.nz),
+                                    form, args.explicit_kernel)
         m["step_roofline"] = {"bytes_per_step": sb,
                               "achieved_gbs": sb / (m["ms"] / args.steps / 1e3) / 1e9,
                               "frac_of_hbm": sb / (m["ms"] / args.steps / 1e3) / 1e9 / hbm}

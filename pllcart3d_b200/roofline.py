@@ -30,25 +30,36 @@ KERNEL_WORDS = {
     "div_rhs": 4,        # u, v, w ; rhs
     "dct_gemm": 2,       # one dense pass: in ; out (per launch)
     "dct_umma": 2,
+    "dct_fft": 2,        # one FFT pass: in ; out
     "poisson_x": 2,
     "project": 17,       # u v w phi mu(4) pg(3) ; u v w pg(3)
     "cfl": 3,
 }
 
 
-# kernel families (one CUDA kernel template each) of the per-launch labels
+# kernel families (one CUDA kernel template each) of the per-launch labels in
+# the FP64 and mixed64 forms (explicit="tma", the default on these forms)
 FAMILY = {
-    "explicit_c": "k_explicit", "explicit_u": "k_explicit", "explicit_v": "k_explicit",
-    "explicit_w": "k_explicit",
-    "adi_y_c": "k_line_pf (y)", "adi_y_u": "k_line_pf (y)", "adi_y_v": "k_line_pf (y)",
+    "explicit_c": "k_explicit_tma", "explicit_u": "k_explicit_tma", "explicit_v": "k_explicit_tma",
+    "explicit_w": "k_explicit_tma",
+    "adi_y_c": "k_line_seg (y)", "adi_y_u": "k_line_pf (y)", "adi_y_v": "k_line_pf (y)",
     "adi_y_w": "k_line_pf (y)",
-    "adi_z_c": "k_adi_z_tiled", "adi_z_u": "k_adi_z_tiled", "adi_z_v": "k_adi_z_tiled",
-    "adi_z_w": "k_adi_z_tiled",
+    "adi_z_c": "k_adi_z_part", "adi_z_u": "k_adi_z_part", "adi_z_v": "k_adi_z_part",
+    "adi_z_w": "k_adi_z_part",
     "adi_x_c": "k_line_pf (x)", "adi_x_u": "k_line_pf (x)", "adi_x_v": "k_line_pf (x)",
     "adi_x_w": "k_line_pf (x)",
-    "viscosity": "k_viscosity", "div_rhs": "k_div_rhs", "dct_gemm": "k_gemm_dmma",
-    "dct_umma": "k_dct_umma", "poisson_x": "k_poisson_x", "project": "k_project", "cfl": "k_cfl",
+    "viscosity": "k_viscosity2", "div_rhs": "k_div_rhs2", "dct_fft": "k_dct_fft",
+    "poisson_x": "k_poisson_x", "project": "k_project2", "cfl": "k_cfl",
 }
+
+# the exact FP64 form's kernels where they differ (bit-reproducible order of
+# operations: no paired-cell kernels, DMMA DCT, tiled z solve)
+FAMILY_EXACT = dict(FAMILY, **{
+    "explicit_c": "k_explicit", "explicit_u": "k_explicit", "explicit_v": "k_explicit",
+    "explicit_w": "k_explicit", "adi_y_c": "k_line_pf (y)",
+    "adi_z_c": "k_adi_z_tiled", "adi_z_u": "k_adi_z_tiled", "adi_z_v": "k_adi_z_tiled",
+    "adi_z_w": "k_adi_z_tiled",
+    "viscosity": "k_viscosity", "div_rhs": "k_div_rhs", "dct_gemm": "k_gemm_dmma", "project": "k_project"})
 
 # the precision form's kernels where they differ from the FP64 form's
 FAMILY_FP32 = {
@@ -64,10 +75,18 @@ FAMILY_FP32 = {
 }
 
 
-def family(label: str, precision: str = "fp64"):
-    """Kernel (family) that runs `label` in the given form, or None."""
+def family(label: str, precision: str = "fp64", form: str = None, explicit: str = "auto"):
+    """Kernel (family) that runs `label` in the given form, or None.  `form`
+    is "fp64x" for the exact form; `explicit` is the Solver's explicit_kernel
+    ("direct" runs the FP64 forms' explicit operator as k_explicit)."""
     if precision == "fp32" and label in FAMILY_FP32:
+        if explicit == "tma" and label.startswith("explicit_"):
+            return "k_explicit_tma"
         return FAMILY_FP32[label]
+    if form == "fp64x":
+        return FAMILY_EXACT.get(label)
+    if explicit == "direct" and label.startswith("explicit_"):
+        return "k_explicit"
     return FAMILY.get(label)
 
 

@@ -13,15 +13,24 @@ def test_every_label_has_words_and_family():
     for lab in LABELS:
         assert roofline.KERNEL_WORDS[lab] > 0, lab
         assert roofline.family(lab, "fp64"), lab
+        assert roofline.family(lab, "fp64", "fp64x"), lab
         assert roofline.family(lab, "fp32"), lab
 
 
-def test_precision_form_names_its_kernels():
-    assert roofline.family("explicit_u", "fp64") == "k_explicit"
+def test_each_form_names_its_kernels():
+    assert roofline.family("explicit_u", "fp64") == "k_explicit_tma"
+    assert roofline.family("explicit_u", "fp64", "mixed64", "direct") == "k_explicit"
+    assert roofline.family("explicit_u", "fp64", "fp64x") == "k_explicit"
+    assert roofline.family("adi_z_u", "fp64") == "k_adi_z_part"
+    assert roofline.family("adi_z_u", "fp64", "fp64x") == "k_adi_z_tiled"
+    assert roofline.family("adi_y_c", "fp64") == "k_line_seg (y)"
+    assert roofline.family("dct_fft", "fp64") == "k_dct_fft"
+    assert roofline.family("dct_gemm", "fp64", "fp64x") == "k_gemm_dmma"
     assert roofline.family("explicit_u", "fp32") == "k_explicit2"
+    assert roofline.family("explicit_u", "fp32", "mixed", "tma") == "k_explicit_tma"
     assert roofline.family("adi_x_c", "fp32") == "k_line_seg (x)"
     assert roofline.family("adi_z_w", "fp32") == "k_adi_z_part"
-    assert roofline.family("dct_gemm", "fp32") == "k_gemm_dmma"   # no precision-form override
+    assert roofline.family("dct_gemm", "fp32", "fp64x") == "k_gemm_dmma"   # no precision-form override
     assert roofline.family("not_a_label", "fp32") is None
 
 
@@ -53,5 +62,7 @@ def test_bench_roofline_picks_the_largest_family():
     assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-12
     assert abs(r["traffic"] - bench.TRAFFIC_RATIO[("k_explicit2", "fp32")] * alg) < 1.0
     assert abs(r["share_of_step"] - 12.0 / 16.0) < 1e-12
-    r64 = bench.roofline_of(kernels, 2, cells, "fp64")
-    assert r64["kernel"] == "k_explicit"
+    r64 = bench.roofline_of(kernels, 2, cells, "fp64", form="mixed64")
+    assert r64["kernel"] == "k_explicit_tma"
+    assert abs(r64["traffic"] - bench.TRAFFIC_RATIO[("k_explicit_tma", "fp64")]
+               * roofline.kernel_bytes_per_launch("explicit_u", cells, "fp64")) < 1.0
