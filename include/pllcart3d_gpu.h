@@ -261,10 +261,13 @@ int pllgpu_set_tuning(pllgpu_ctx *ctx, int explicit_variant, int line_variant);
 
 /* ---- ensembles ------------------------------------------------------------
  * n independent runs (each its own grid and parameters, params[i]) on one
- * device, advanced together: one CUDA graph per step holds every member's
- * step as a parallel branch.  Members are ordinary contexts
- * (pllgpu_ensemble_member): set their fields and read them with the calls
- * above.  Every member computes exactly what it computes alone. */
+ * device, advanced together by one CUDA graph launch per step.  Members
+ * whose steps issue the same launches (the same grid and form) form a
+ * class; the graph holds one branch per class and, by default, one launch
+ * per stage for the whole class (each member reading its own arguments from
+ * a device table).  Members are ordinary contexts (pllgpu_ensemble_member):
+ * set their fields and read them with the calls above.  Every member
+ * computes exactly what it computes alone.  No reference counterpart. */
 typedef struct pllgpu_ensemble pllgpu_ensemble;
 pllgpu_ensemble *pllgpu_ensemble_create(int n, const pllgpu_params *params,
                                         int device);
@@ -276,6 +279,15 @@ int pllgpu_ensemble_steps(pllgpu_ensemble *ens, int nsteps);
 int pllgpu_ensemble_autotune(pllgpu_ensemble *ens, int trial_steps,
                              int *steps_done);
 int pllgpu_ensemble_launches_per_step(const pllgpu_ensemble *ens);
+/* mode 1 (the default): one launch per stage and class; k >= 2: classes
+ * split into groups of at most k members, one launch per stage and group;
+ * 0: every member's own launches as its own branch.  Returns the previous
+ * mode (negative: invalid arguments); the graphs are rebuilt on the next
+ * steps call. */
+int pllgpu_ensemble_set_batching(pllgpu_ensemble *ens, int mode);
+/* branches (classes, or groups of a class) of the graphs last built (0
+ * before the first steps call) */
+int pllgpu_ensemble_classes(const pllgpu_ensemble *ens);
 
 /* the whole state of src (fields of both buffer roles, viscosity,
  * pressure gradient, phi, device scalars) into dst, device to device; both

@@ -135,6 +135,8 @@ def lib():
     L.pllgpu_ensemble_steps.argtypes = [_VP, _I]
     L.pllgpu_ensemble_autotune.argtypes = [_VP, _I, _PI]
     L.pllgpu_ensemble_launches_per_step.argtypes = [_VP]
+    L.pllgpu_ensemble_set_batching.argtypes = [_VP, _I]
+    L.pllgpu_ensemble_classes.argtypes = [_VP]
     L.pllgpu_pack_cells.argtypes = [_VP, _VP]
     L.pllgpu_unpack_cells.argtypes = [_VP, _VP]
     L.pllgpu_copy_state.argtypes = [_VP, _VP]
@@ -159,5 +161,6 @@ EXPORTED_SYMBOLS = [
     "pllgpu_ensemble_create", "pllgpu_ensemble_destroy", "pllgpu_ensemble_size",
     "pllgpu_ensemble_member", "pllgpu_ensemble_start", "pllgpu_ensemble_steps",
     "pllgpu_ensemble_autotune", "pllgpu_ensemble_launches_per_step",
+    "pllgpu_ensemble_set_batching", "pllgpu_ensemble_classes",
     "pllgpu_pack_cells", "pllgpu_unpack_cells", "pllgpu_copy_state",
 ]

@@ -14,6 +14,7 @@ Run ``python -m pllcart3d_b200.build`` or call :func:`build`.
 
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -33,15 +34,19 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17",
 
 # per-source contraction: the exact FP64 form (form_f64x.cu) and everything
 # the drop-in layer's primitives run reproduce the reference's operation
-# order, so no multiply-add is contracted there; the FP64 form (form_f64.cu)
-# and the precision form's FP32 kernels (form_f32.cu) are free to contract.
+# order, so no multiply-add is contracted there; the FP64 forms (form_f64.cu,
+# form_f64m.cu) are free to contract.  The precision form's FP32 kernels
+# (form_f32.cu) fuse only where the source asks (fma, the paired FP32x2
+# intrinsics): a contraction the compiler chooses may differ between a
+# kernel and its member-batched copy, whose results must be the same bits.
 CU_SOURCES = {"runtime.cu": "--fmad=false", "form_f64.cu": "--fmad=true", "form_f64x.cu": "--fmad=false",
               "form_f64m.cu": "--fmad=true",
-              "form_f32.cu": "--fmad=true", "primitives.cu": "--fmad=false",
+              "form_f32.cu": "--fmad=false", "primitives.cu": "--fmad=false",
               "noalloc.cu": "--fmad=false", "io.cu": "--fmad=false",
               "wave.cu": "--fmad=false", "ensemble.cu": "--fmad=false"}
 HEADERS = ["common.cuh", "step_kernels.cuh", "aux_kernels.cuh", "dct_kernels.cuh", "host_util.h",
-           "ctx.cuh", "host_common.cuh", "orchestrate.cuh", "forms.h", "umma_dct.cuh", "fft_dct.cuh", "explicit_tma.cuh"]
+           "ctx.cuh", "host_common.cuh", "orchestrate.cuh", "forms.h", "umma_dct.cuh", "fft_dct.cuh", "explicit_tma.cuh",
+           "batch.cuh"]
 
 
 def _nvcc() -> str:
@@ -63,15 +68,20 @@ def build(force: bool = False, verbose: bool = False) -> str:
     deps.append(os.path.join(INC, "pllcart3d_gpu.h"))
     deps.append(__file__)
     if force or _stale(LIB, deps):
-        objs = []
+        # the translation units compile in parallel (the form units dominate)
+        cmds, objs = [], []
         for src, fmad in CU_SOURCES.items():
             obj = os.path.join(CSRC, src.replace(".cu", ".o"))
-            cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, fmad, "-I", INC, "-c",
-                   os.path.join(CSRC, src), "-o", obj]
-            if verbose:
-                print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
+            cmds.append([_nvcc(), *ARCH, *NVCC_FLAGS, *fmad.split(), "-I", INC, "-c", os.path.join(CSRC, src), "-o", obj])
             objs.append(obj)
+        if verbose:
+            for cmd in cmds:
+                print(" ".join(cmd))
+        workers = max(1, min(len(cmds), os.cpu_count() or 1))
+        with concurrent.futures.ThreadPoolExecutor(workers) as ex:
+            for r in list(ex.map(lambda c: subprocess.run(c), cmds)):
+                if r.returncode != 0:
+                    raise subprocess.CalledProcessError(r.returncode, r.args)
         cmd = [_nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs]
         subprocess.run(cmd, check=True)
         for o in objs:

@@ -41,7 +41,8 @@ constexpr int VISC_NI = 4;
 // come from the previous plane's registers.  Every point read lies inside the
 // padded box's allocation (i >= is-1 >= 2), whether or not its value is used.
 template <typename real>
-__global__ void __launch_bounds__(128) k_viscosity(Geo G, Rng R, Consts K, int nmvp,
+__device__ __forceinline__ void k_viscosity_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng R, Consts K, int nmvp,
                                                    const real* __restrict__ cn, real* __restrict__ mc,
                                                    real* __restrict__ mxy, real* __restrict__ mxz,
                                                    real* __restrict__ myz, const double* __restrict__ scal)
@@ -72,6 +73,19 @@ __global__ void __launch_bounds__(128) k_viscosity(Geo G, Rng R, Consts K, int n
         pz = cz;
     }
 }
+template <typename real>
+__global__ void __launch_bounds__(128) k_viscosity(Geo G, Rng R, Consts K, int nmvp,
+                                                   const real* __restrict__ cn, real* __restrict__ mc,
+                                                   real* __restrict__ mxy, real* __restrict__ mxz,
+                                                   real* __restrict__ myz, const double* __restrict__ scal)
+{
+    k_viscosity_run<real>(blockIdx, gridDim, G, R, K, nmvp, cn, mc, mxy, mxz, myz, scal);
+}
+template <typename real>
+struct k_viscosity_b {
+    static constexpr auto run = &k_viscosity_run<real>;
+    static constexpr int maxt = 128, minb = 0;
+};
 
 // The exponential law on cell pairs (k, k+32): the precision form with
 // packed FP32x2 arithmetic (the averages and exponents; __expf per value),
@@ -79,7 +93,8 @@ __global__ void __launch_bounds__(128) k_viscosity(Geo G, Rng R, Consts K, int n
 // VISC_NI planes as k_viscosity.  A second cell past NZ reads the slack past
 // the array and stores nothing.  Grid: x over k in tiles of 64.
 template <typename real>
-__global__ void __launch_bounds__(128) k_viscosity2(Geo G, Rng R, Consts K, const real* __restrict__ cn,
+__device__ __forceinline__ void k_viscosity2_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng R, Consts K, const real* __restrict__ cn,
                                                     real* __restrict__ mc, real* __restrict__ mxy,
                                                     real* __restrict__ mxz, real* __restrict__ myz)
 {
@@ -131,13 +146,26 @@ __global__ void __launch_bounds__(128) k_viscosity2(Geo G, Rng R, Consts K, cons
         pz = cz;
     }
 }
+template <typename real>
+__global__ void __launch_bounds__(128) k_viscosity2(Geo G, Rng R, Consts K, const real* __restrict__ cn,
+                                                    real* __restrict__ mc, real* __restrict__ mxy,
+                                                    real* __restrict__ mxz, real* __restrict__ myz)
+{
+    k_viscosity2_run<real>(blockIdx, gridDim, G, R, K, cn, mc, mxy, mxz, myz);
+}
+template <typename real>
+struct k_viscosity2_b {
+    static constexpr auto run = &k_viscosity2_run<real>;
+    static constexpr int maxt = 128, minb = 0;
+};
 
 // find_cfl (pllcart3d.c:3095-3118): max over interior cells of
 // |u|/dx+|v|/dy+|w|/dz at cell centres, reduced exactly through the bit
 // pattern of non-negative doubles; a NaN/Inf raises ST_NAN (the reference's
 // NaN guard lives in find_max, pllcart3d.c:3568-3588)
 template <typename real>
-__global__ void __launch_bounds__(256) k_cfl(Geo G, Rng R, Consts K, const real* __restrict__ u,
+__device__ __forceinline__ void k_cfl_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng R, Consts K, const real* __restrict__ u,
                                              const real* __restrict__ v, const real* __restrict__ w,
                                              double* scal, int* status)
 {
@@ -170,10 +198,23 @@ __global__ void __launch_bounds__(256) k_cfl(Geo G, Rng R, Consts K, const real*
             atomicMax((unsigned long long*)(scal + S_CFLMAX), (unsigned long long)__double_as_longlong(m));
     }
 }
+template <typename real>
+__global__ void __launch_bounds__(256) k_cfl(Geo G, Rng R, Consts K, const real* __restrict__ u,
+                                             const real* __restrict__ v, const real* __restrict__ w,
+                                             double* scal, int* status)
+{
+    k_cfl_run<real>(blockIdx, gridDim, G, R, K, u, v, w, scal, status);
+}
+template <typename real>
+struct k_cfl_b {
+    static constexpr auto run = &k_cfl_run<real>;
+    static constexpr int maxt = 256, minb = 0;
+};
 
 // dt = min(CFLmax / max, Timestep), pllcart3d.c:159-160, 3115; clears the
 // reduction slot for the next step
-static __global__ void k_dt(Consts K, double* scal)
+static __device__ __forceinline__ void k_dt_run(const uint3 blockIdx, const dim3 gridDim,
+    Consts K, double* scal)
 {
     double maxall = __longlong_as_double((long long)*(unsigned long long*)(scal + S_CFLMAX));
     double cfldt = K.CFLmax / maxall;
@@ -182,13 +223,22 @@ static __global__ void k_dt(Consts K, double* scal)
     scal[S_DT] = (cfldt < ts) ? cfldt : ts;
     *(unsigned long long*)(scal + S_CFLMAX) = 0ull;
 }
+static __global__ void k_dt(Consts K, double* scal)
+{
+    k_dt_run(blockIdx, gridDim, K, scal);
+}
+struct k_dt_b {
+    static constexpr auto run = &k_dt_run;
+    static constexpr int maxt = 0, minb = 0;
+};
 
 // inflow/outflow trapezoid fluxes of velo_correction (pllcart3d.c:2171-2223):
 // per y row a sequential sum over z of 0.5*dz*(u_k+u_{k-1}) from k=ks+1,
 // then a sequential sum over y of 0.5*dy*(q_{j-1}+q_j) from j=js+1 (wall
 // half-cells excluded), in the reference's order.  One block.
 template <typename real>
-__global__ void __launch_bounds__(512) k_flux(Geo G, Rng Ru, Consts K, const real* __restrict__ u,
+__device__ __forceinline__ void k_flux_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng Ru, Consts K, const real* __restrict__ u,
                                               double* scal)
 {
     extern __shared__ double qk[];  // 2 * NY
@@ -216,6 +266,17 @@ __global__ void __launch_bounds__(512) k_flux(Geo G, Rng Ru, Consts K, const rea
         scal[S_DEFICIT] = (qin - qout) / K.area;
     }
 }
+template <typename real>
+__global__ void __launch_bounds__(512) k_flux(Geo G, Rng Ru, Consts K, const real* __restrict__ u,
+                                              double* scal)
+{
+    k_flux_run<real>(blockIdx, gridDim, G, Ru, K, u, scal);
+}
+template <typename real>
+struct k_flux_b {
+    static constexpr auto run = &k_flux_run<real>;
+    static constexpr int maxt = 512, minb = 0;
+};
 
 // The precision form's Poisson right-hand side (k_div_rhs mode 0) on cell
 // pairs (k, k+32) with packed FP32x2 arithmetic, each thread walking
@@ -224,7 +285,8 @@ __global__ void __launch_bounds__(512) k_flux(Geo G, Rng Ru, Consts K, const rea
 constexpr int DIV_NI = 4;
 
 template <typename real>
-__global__ void __launch_bounds__(128) k_div_rhs2(Geo G, Rng R, Consts K, const real* __restrict__ u,
+__device__ __forceinline__ void k_div_rhs2_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng R, Consts K, const real* __restrict__ u,
                                                   const real* __restrict__ v, const real* __restrict__ w,
                                                   real* __restrict__ rhs, const double* __restrict__ scal,
                                                   double alpha)
@@ -256,6 +318,19 @@ __global__ void __launch_bounds__(128) k_div_rhs2(Geo G, Rng R, Consts K, const 
         u0 = u1;
     }
 }
+template <typename real>
+__global__ void __launch_bounds__(128) k_div_rhs2(Geo G, Rng R, Consts K, const real* __restrict__ u,
+                                                  const real* __restrict__ v, const real* __restrict__ w,
+                                                  real* __restrict__ rhs, const double* __restrict__ scal,
+                                                  double alpha)
+{
+    k_div_rhs2_run<real>(blockIdx, gridDim, G, R, K, u, v, w, rhs, scal, alpha);
+}
+template <typename real>
+struct k_div_rhs2_b {
+    static constexpr auto run = &k_div_rhs2_run<real>;
+    static constexpr int maxt = 128, minb = 0;
+};
 
 // The precision form's CFL scan: cell pairs (k, k+32), CFL_NI planes per
 // thread, the per-cell speed sum in FP64 (the reciprocal spacings multiply:
@@ -265,7 +340,8 @@ __global__ void __launch_bounds__(128) k_div_rhs2(Geo G, Rng R, Consts K, const 
 // the slack past the arrays and is left out.
 constexpr int CFL_NI = 8;
 
-__global__ void __launch_bounds__(256) k_cfl2(Geo G, Rng R, Consts K, const float* __restrict__ u,
+__device__ __forceinline__ void k_cfl2_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng R, Consts K, const float* __restrict__ u,
                                               const float* __restrict__ v, const float* __restrict__ w, double* scal,
                                               int* status)
 {
@@ -314,6 +390,16 @@ __global__ void __launch_bounds__(256) k_cfl2(Geo G, Rng R, Consts K, const floa
             atomicMax((unsigned long long*)(scal + S_CFLMAX), (unsigned long long)__double_as_longlong(m));
     }
 }
+__global__ void __launch_bounds__(256) k_cfl2(Geo G, Rng R, Consts K, const float* __restrict__ u,
+                                              const float* __restrict__ v, const float* __restrict__ w, double* scal,
+                                              int* status)
+{
+    k_cfl2_run(blockIdx, gridDim, G, R, K, u, v, w, scal, status);
+}
+struct k_cfl2_b {
+    static constexpr auto run = &k_cfl2_run;
+    static constexpr int maxt = 256, minb = 0;
+};
 
 // Last-block ticket: every block's results are written and fenced before it
 // takes a ticket; the block that takes the last one reads them all and
@@ -334,7 +420,8 @@ __device__ __forceinline__ bool last_block(unsigned* ticket)
 // bits): one warp per row of either plane, lane l summing the terms k =
 // ks+1+l, ks+1+l+32, ... and a fixed shuffle tree; the last block forms the
 // sum over y the same way from the row sums.  Blocks of 1024 threads.
-__global__ void __launch_bounds__(1024) k_flux3(Geo G, Rng Ru, Consts K, const float* __restrict__ u, double* red,
+__device__ __forceinline__ void k_flux3_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng Ru, Consts K, const float* __restrict__ u, double* red,
                                                 unsigned* ticket, double* scal)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -371,6 +458,15 @@ __global__ void __launch_bounds__(1024) k_flux3(Geo G, Rng Ru, Consts K, const f
         }
     }
 }
+__global__ void __launch_bounds__(1024) k_flux3(Geo G, Rng Ru, Consts K, const float* __restrict__ u, double* red,
+                                                unsigned* ticket, double* scal)
+{
+    k_flux3_run(blockIdx, gridDim, G, Ru, K, u, red, ticket, scal);
+}
+struct k_flux3_b {
+    static constexpr auto run = &k_flux3_run;
+    static constexpr int maxt = 1024, minb = 0;
+};
 
 // bulk_velo (pllcart3d.c:3381-3398): the signed value of the first (j-major,
 // k-minor) entry of largest |u| on the face i = iend; 0 if all are 0.  Over
@@ -378,7 +474,8 @@ __global__ void __launch_bounds__(1024) k_flux3(Geo G, Rng Ru, Consts K, const f
 // index among equal values, the last block the block partials; the result
 // does not depend on the order.
 template <typename real>
-__global__ void __launch_bounds__(1024) k_bulk2(Geo G, Rng R, const real* __restrict__ u, double* red,
+__device__ __forceinline__ void k_bulk2_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng R, const real* __restrict__ u, double* red,
                                                unsigned* ticket, double* scal)
 {
     const int nyz = (R.je - R.js + 1) * (R.ke - R.ks + 1), nk = R.ke - R.ks + 1;
@@ -438,12 +535,24 @@ __global__ void __launch_bounds__(1024) k_bulk2(Geo G, Rng R, const real* __rest
         }
     }
 }
+template <typename real>
+__global__ void __launch_bounds__(1024) k_bulk2(Geo G, Rng R, const real* __restrict__ u, double* red,
+                                               unsigned* ticket, double* scal)
+{
+    k_bulk2_run<real>(blockIdx, gridDim, G, R, u, red, ticket, scal);
+}
+template <typename real>
+struct k_bulk2_b {
+    static constexpr auto run = &k_bulk2_run<real>;
+    static constexpr int maxt = 1024, minb = 0;
+};
 
 // divergence (pllcart3d.c:1983-1999) scaled by Re/(dt alpha)
 // (phisolver_dct L2010-2024) into the compact [x][y][z] Poisson buffer.
 // With `div_out` set, the unscaled divergence also goes to the padded field.
 template <typename real>
-__global__ void __launch_bounds__(128) k_div_rhs(Geo G, Rng R, Consts K, const real* __restrict__ u,
+__device__ __forceinline__ void k_div_rhs_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng R, Consts K, const real* __restrict__ u,
                                                  const real* __restrict__ v, const real* __restrict__ w,
                                                  const real* __restrict__ div_in, real* __restrict__ div_out,
                                                  real* __restrict__ rhs, const double* __restrict__ scal,
@@ -472,6 +581,20 @@ __global__ void __launch_bounds__(128) k_div_rhs(Geo G, Rng R, Consts K, const r
     const long c = ((long)(i - R.is) * (R.je - R.js + 1) + (j - R.js)) * (long)(R.ke - R.ks + 1) + (k - R.ks);
     rhs[c] = fac * d;
 }
+template <typename real>
+__global__ void __launch_bounds__(128) k_div_rhs(Geo G, Rng R, Consts K, const real* __restrict__ u,
+                                                 const real* __restrict__ v, const real* __restrict__ w,
+                                                 const real* __restrict__ div_in, real* __restrict__ div_out,
+                                                 real* __restrict__ rhs, const double* __restrict__ scal,
+                                                 double alpha, int mode)
+{
+    k_div_rhs_run<real>(blockIdx, gridDim, G, R, K, u, v, w, div_in, div_out, rhs, scal, alpha, mode);
+}
+template <typename real>
+struct k_div_rhs_b {
+    static constexpr auto run = &k_div_rhs_run<real>;
+    static constexpr int maxt = 128, minb = 0;
+};
 
 // x-direction tridiagonal of each (ky,kz) Poisson mode (phisolver_dct
 // pllcart3d.c:2040-2091): a = c = 1/dx^2, b = -2/dx^2 + lam_y + lam_z,
@@ -482,7 +605,8 @@ __global__ void __launch_bounds__(128) k_div_rhs(Geo G, Rng R, Consts K, const r
 // but the solve, the eigenvalue division and the zero mode are FP64, with
 // c' and the eliminated rhs in FP64 scratch.
 template <typename T>
-__global__ void __launch_bounds__(128) k_poisson_x(int nx, int ny, int nz, Consts K,
+__device__ __forceinline__ void k_poisson_x_run(const uint3 blockIdx, const dim3 gridDim,
+    int nx, int ny, int nz, Consts K,
                                                    const double* __restrict__ lam_y,
                                                    const double* __restrict__ lam_z,
                                                    T* __restrict__ hat, double* __restrict__ cc,
@@ -574,12 +698,27 @@ __global__ void __launch_bounds__(128) k_poisson_x(int nx, int ny, int nz, Const
         }
     }
 }
+template <typename T>
+__global__ void __launch_bounds__(128) k_poisson_x(int nx, int ny, int nz, Consts K,
+                                                   const double* __restrict__ lam_y,
+                                                   const double* __restrict__ lam_z,
+                                                   T* __restrict__ hat, double* __restrict__ cc,
+                                                   double* __restrict__ rr, int kz_major = 0)
+{
+    k_poisson_x_run<T>(blockIdx, gridDim, nx, ny, nz, K, lam_y, lam_z, hat, cc, rr, kz_major);
+}
+template <typename T>
+struct k_poisson_x_b {
+    static constexpr auto run = &k_poisson_x_run<T>;
+    static constexpr int maxt = 128, minb = 0;
+};
 
 // update_phi_ghosts (pllcart3d.c:2758-2807): Neumann copies on the six
 // faces; FACE 0: z faces over (i,j), 1: y faces over (i,k), 2: x faces over
 // (j,k)
 template <int FACE, typename real>
-__global__ void k_phi_ghosts(Geo G, Rng R, real* __restrict__ p)
+__device__ __forceinline__ void k_phi_ghosts_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng R, real* __restrict__ p)
 {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     const int b = blockIdx.y;
@@ -604,6 +743,16 @@ __global__ void k_phi_ghosts(Geo G, Rng R, real* __restrict__ p)
         p[base + (long)(R.ie + 1) * sx] = p[base + (long)R.ie * sx];
     }
 }
+template <int FACE, typename real>
+__global__ void k_phi_ghosts(Geo G, Rng R, real* __restrict__ p)
+{
+    k_phi_ghosts_run<FACE, real>(blockIdx, gridDim, G, R, p);
+}
+template <int FACE, typename real>
+struct k_phi_ghosts_b {
+    static constexpr auto run = &k_phi_ghosts_run<FACE, real>;
+    static constexpr int maxt = 0, minb = 0;
+};
 
 // planes of i one k_project thread walks
 constexpr int PROJECT_NI = 1;
@@ -642,7 +791,8 @@ __device__ __forceinline__ real pg_update(const Consts& K, const Geo& G, const r
 // (a thread's own u, v, w and ghosts outside the walked range), so the loads
 // of both planes may all be in flight before the first store.
 template <typename real>
-__global__ void __launch_bounds__(128) k_project(Geo G, Rng Rg, Rng Ru, Rng Rv, Rng Rw, Consts K,
+__device__ __forceinline__ void k_project_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng Rg, Rng Ru, Rng Rv, Rng Rw, Consts K,
         real* __restrict__ u, real* __restrict__ v, real* __restrict__ w,
         real* __restrict__ pgu, real* __restrict__ pgv, real* __restrict__ pgw,
         const real* __restrict__ phi, const real* __restrict__ mc, const real* __restrict__ mxy,
@@ -708,6 +858,22 @@ __global__ void __launch_bounds__(128) k_project(Geo G, Rng Rg, Rng Ru, Rng Rv, 
         }
     }
 }
+template <typename real>
+__global__ void __launch_bounds__(128) k_project(Geo G, Rng Rg, Rng Ru, Rng Rv, Rng Rw, Consts K,
+        real* __restrict__ u, real* __restrict__ v, real* __restrict__ w,
+        real* __restrict__ pgu, real* __restrict__ pgv, real* __restrict__ pgw,
+        const real* __restrict__ phi, const real* __restrict__ mc, const real* __restrict__ mxy,
+        const real* __restrict__ mxz, const real* __restrict__ myz, const double* __restrict__ scal,
+        double alpha, int do_correct, int do_ghosts, int do_pg)
+{
+    k_project_run<real>(blockIdx, gridDim, G, Rg, Ru, Rv, Rw, K, u, v, w, pgu, pgv, pgw, phi, mc, mxy, mxz, myz, scal,
+                        alpha, do_correct, do_ghosts, do_pg);
+}
+template <typename real>
+struct k_project_b {
+    static constexpr auto run = &k_project_run<real>;
+    static constexpr int maxt = 128, minb = 0;
+};
 
 // The precision form's projection on cell pairs (k, k+32) with packed FP32x2
 // arithmetic, as k_explicit2: the same fused correction, ghosts and pressure
@@ -739,7 +905,8 @@ __device__ __forceinline__ typename PairOf<real>::type pg_update2(const Consts& 
 }
 
 template <typename real>
-__global__ void __launch_bounds__(128, sizeof(real) == 4 ? 16 : 8) k_project2(Geo G, Rng Rg, Rng Ru, Rng Rv, Rng Rw,
+__device__ __forceinline__ void k_project2_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng Rg, Rng Ru, Rng Rv, Rng Rw,
         Consts K, real* __restrict__ u, real* __restrict__ v, real* __restrict__ w,
         real* __restrict__ pgu, real* __restrict__ pgv, real* __restrict__ pgw,
         const real* __restrict__ phi, MuPtrs<real> mu, const double* __restrict__ scal,
@@ -821,6 +988,21 @@ __global__ void __launch_bounds__(128, sizeof(real) == 4 ? 16 : 8) k_project2(Ge
         }
     }
 }
+template <typename real>
+__global__ void __launch_bounds__(128, sizeof(real) == 4 ? 16 : 8) k_project2(Geo G, Rng Rg, Rng Ru, Rng Rv, Rng Rw,
+        Consts K, real* __restrict__ u, real* __restrict__ v, real* __restrict__ w,
+        real* __restrict__ pgu, real* __restrict__ pgv, real* __restrict__ pgw,
+        const real* __restrict__ phi, MuPtrs<real> mu, const double* __restrict__ scal,
+        double alpha, int do_correct, int do_ghosts, int do_pg)
+{
+    k_project2_run<real>(blockIdx, gridDim, G, Rg, Ru, Rv, Rw, K, u, v, w, pgu, pgv, pgw, phi, mu, scal, alpha,
+                         do_correct, do_ghosts, do_pg);
+}
+template <typename real>
+struct k_project2_b {
+    static constexpr auto run = &k_project2_run<real>;
+    static constexpr int maxt = 128, minb = sizeof(real) == 4 ? 16 : 8, bminb = 8;
+};
 
 // The precision form's mode solve with a third of k_poisson_x's scratch
 // traffic: the same FP64 Thomas recurrences per (ky, kz) mode, but the
@@ -832,7 +1014,8 @@ __global__ void __launch_bounds__(128, sizeof(real) == 4 ? 16 : 8) k_project2(Ge
 // of two divisions.  16.5 bytes per cell instead of 40.
 constexpr int PX_CK = 16;
 
-__global__ void __launch_bounds__(128) k_poisson_x2(int nx, int ny, int nz, Consts K,
+__device__ __forceinline__ void k_poisson_x2_run(const uint3 blockIdx, const dim3 gridDim,
+    int nx, int ny, int nz, Consts K,
                                                     const double* __restrict__ lam_y,
                                                     const double* __restrict__ lam_z, float* __restrict__ hat,
                                                     float* __restrict__ rr, double* __restrict__ ck, int kz_major)
@@ -907,6 +1090,17 @@ __global__ void __launch_bounds__(128) k_poisson_x2(int nx, int ny, int nz, Cons
         }
     }
 }
+__global__ void __launch_bounds__(128) k_poisson_x2(int nx, int ny, int nz, Consts K,
+                                                    const double* __restrict__ lam_y,
+                                                    const double* __restrict__ lam_z, float* __restrict__ hat,
+                                                    float* __restrict__ rr, double* __restrict__ ck, int kz_major)
+{
+    k_poisson_x2_run(blockIdx, gridDim, nx, ny, nz, K, lam_y, lam_z, hat, rr, ck, kz_major);
+}
+struct k_poisson_x2_b {
+    static constexpr auto run = &k_poisson_x2_run;
+    static constexpr int maxt = 128, minb = 0;
+};
 
 // slope_parameter (pllcart3d.c:722-840) on one rank: bisection for the
 // non-monotonic viscosity law's cm from c along the x line closest to

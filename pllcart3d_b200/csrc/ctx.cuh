@@ -14,6 +14,7 @@
 
 #include "../../include/pllcart3d_gpu.h"
 #include "aux_kernels.cuh"
+#include "batch.cuh"
 #include "common.cuh"
 #include "dct_kernels.cuh"
 #include "host_util.h"
@@ -90,6 +91,7 @@ struct pllgpu_ctx {
     int launches_per_step = 0;
     int counting = 0;
     bool profiling = false;
+    std::vector<pll::LaunchRec*>* rec = nullptr;   // recording: launches are stored, not issued
     std::vector<cudaEvent_t> ev_pool;
     std::vector<const char*> ev_label;
     std::vector<void*> allocs;

@@ -27,7 +27,8 @@ struct GemmDesc {
 // acc = acc + a*b, from 0 (the summation order of a sequential loop).
 // 64x64 output tile per 256-thread block, 4x4 outputs per thread.
 template <typename real>
-__global__ void __launch_bounds__(256) k_gemm_seq(GemmDesc d, const real* __restrict__ A,
+__device__ __forceinline__ void k_gemm_seq_run(const uint3 blockIdx, const dim3 gridDim,
+    GemmDesc d, const real* __restrict__ A,
                                                   const real* __restrict__ B, real* __restrict__ C)
 {
     constexpr int TM = 64, TN = 64, TK = 16;
@@ -86,6 +87,17 @@ __global__ void __launch_bounds__(256) k_gemm_seq(GemmDesc d, const real* __rest
         }
     }
 }
+template <typename real>
+__global__ void __launch_bounds__(256) k_gemm_seq(GemmDesc d, const real* __restrict__ A,
+                                                  const real* __restrict__ B, real* __restrict__ C)
+{
+    k_gemm_seq_run<real>(blockIdx, gridDim, d, A, B, C);
+}
+template <typename real>
+struct k_gemm_seq_b {
+    static constexpr auto run = &k_gemm_seq_run<real>;
+    static constexpr int maxt = 256, minb = 0;
+};
 
 
 // Same contraction on the FP64 tensor cores: mma.sync m8n8k4 .f64 (DMMA),
@@ -100,7 +112,8 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
                  : "d"(a), "d"(b));
 }
 
-static __global__ void __launch_bounds__(256) k_gemm_dmma(GemmDesc d, const double* __restrict__ A,
+static __device__ __forceinline__ void k_gemm_dmma_run(const uint3 blockIdx, const dim3 gridDim,
+    GemmDesc d, const double* __restrict__ A,
                                                    const double* __restrict__ B, double* __restrict__ C)
 {
     constexpr int TM = 64, TN = 64, TK = 16, PAD = 4;
@@ -163,6 +176,15 @@ static __global__ void __launch_bounds__(256) k_gemm_dmma(GemmDesc d, const doub
         }
     }
 }
+static __global__ void __launch_bounds__(256) k_gemm_dmma(GemmDesc d, const double* __restrict__ A,
+                                                   const double* __restrict__ B, double* __restrict__ C)
+{
+    k_gemm_dmma_run(blockIdx, gridDim, d, A, B, C);
+}
+struct k_gemm_dmma_b {
+    static constexpr auto run = &k_gemm_dmma_run;
+    static constexpr int maxt = 256, minb = 0;
+};
 
 
 // Split-TF32 contraction for the precision form: each FP32 operand is split
@@ -193,7 +215,8 @@ __device__ __forceinline__ void mma_tf32_16x8x8(float* d, const uint32_t* a, con
                  : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-static __global__ void __launch_bounds__(256) k_gemm_tf32x3(GemmDesc d, const float* __restrict__ A,
+static __device__ __forceinline__ void k_gemm_tf32x3_run(const uint3 blockIdx, const dim3 gridDim,
+    GemmDesc d, const float* __restrict__ A,
                                                             const float* __restrict__ B, float* __restrict__ C)
 {
     constexpr int TM = 64, TN = 64, TK = 16, PAD = 8;
@@ -269,6 +292,15 @@ static __global__ void __launch_bounds__(256) k_gemm_tf32x3(GemmDesc d, const fl
                 Cb[(long)m * d.sCm + (long)n * d.sCn] = v;
             }
 }
+static __global__ void __launch_bounds__(256) k_gemm_tf32x3(GemmDesc d, const float* __restrict__ A,
+                                                            const float* __restrict__ B, float* __restrict__ C)
+{
+    k_gemm_tf32x3_run(blockIdx, gridDim, d, A, B, C);
+}
+struct k_gemm_tf32x3_b {
+    static constexpr auto run = &k_gemm_tf32x3_run;
+    static constexpr int maxt = 256, minb = 0;
+};
 
 }  // namespace
 }  // namespace pll

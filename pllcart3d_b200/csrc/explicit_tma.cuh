@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(XT_THREADS) k_explicit_tma(const __grid_consta
             A.H[id] = H;
 
             // dt*(gamma H + rho H_old + alpha A q_old + alpha body) (acoef)
-            const real conv = ((real)A.g * H + (real)A.r * hmv);
+            const real conv = rk_comb<real>((real)A.g, H, (real)A.r, hmv);
             real a, c;
             if (VAR == VC) {
                 a = c = (real)K.cdx;

@@ -135,7 +135,8 @@ __device__ __forceinline__ int mperm(int j) { return (j & 1) ? N - 1 - (j >> 1) 
 // consecutive lines per block (inner must be a multiple of 2*FFT_PB).
 // tw: cos / sin of 2 pi m / N (m < N); wq: cos / sin of pi k / (2N) (k < N)
 template <typename real, int N, int KIND, bool CONTIG>
-__global__ void __launch_bounds__(FFT_THREADS) k_dct_fft(FftLines d, const real* __restrict__ in,
+__device__ __forceinline__ void k_dct_fft_run(const uint3 blockIdx, const dim3 gridDim,
+    FftLines d, const real* __restrict__ in,
                                                          real* __restrict__ out, const double2* __restrict__ tw,
                                                          const double2* __restrict__ wq)
 {
@@ -265,6 +266,18 @@ __global__ void __launch_bounds__(FFT_THREADS) k_dct_fft(FftLines d, const real*
         else gout[l + (long)p * d.se_out] = v;
     }
 }
+template <typename real, int N, int KIND, bool CONTIG>
+__global__ void __launch_bounds__(FFT_THREADS) k_dct_fft(FftLines d, const real* __restrict__ in,
+                                                         real* __restrict__ out, const double2* __restrict__ tw,
+                                                         const double2* __restrict__ wq)
+{
+    k_dct_fft_run<real, N, KIND, CONTIG>(blockIdx, gridDim, d, in, out, tw, wq);
+}
+template <typename real, int N, int KIND, bool CONTIG>
+struct k_dct_fft_b {
+    static constexpr auto run = &k_dct_fft_run<real, N, KIND, CONTIG>;
+    static constexpr int maxt = FFT_THREADS, minb = 0;
+};
 
 }  // namespace
 }  // namespace pll

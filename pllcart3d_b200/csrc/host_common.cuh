@@ -25,6 +25,25 @@ int fail(pllgpu_ctx* c, int code)
         }                                                                            \
     } while (0)
 
+// every kernel launch of the step: launched, or recorded while the context
+// records (B: the kernel's batching spec, NoBatch where it has none)
+template <typename B, typename... P, typename... A>
+void go(pllgpu_ctx* ctx, void (*k)(P...), dim3 grid, dim3 blk, size_t smem, A&&... a)
+{
+    if (ctx->rec) {
+        auto* r = new LaunchRecT<B, P...>();
+        r->fn = (const void*)k;
+        r->k = k;
+        r->grid = grid;
+        r->blk = blk;
+        r->smem = smem;
+        tup_fill(r->a, std::forward<A>(a)...);
+        ctx->rec->push_back(r);
+        return;
+    }
+    k<<<grid, blk, smem, ctx->st>>>(std::forward<A>(a)...);
+}
+
 // every kernel launch of the step goes through mark(): it counts launches
 // and, in profiling mode, records an event after the launch so that the
 // device time of each kernel is the gap to the previous event

@@ -72,7 +72,7 @@ bool launch_explicit_tma(pllgpu_ctx* ctx, const ExplicitArgs<real>& A)
     for (int a = 0; a < XtSet<VAR>::NA; ++a)
         if (!field_map<real>(&M.a[a], staged[a], ctx->G, GM::KB1, GM::JB1)) return false;
     const dim3 grid((ctx->G.nz + XT_TK - 1) / XT_TK, (nj(R) + XT_TJ - 1) / XT_TJ, (ni(R) + XT_NI - 1) / XT_NI);
-    k_explicit_tma<VAR, real><<<grid, XT_THREADS, XtSmem<real, VAR>::DYN, ctx->st>>>(M, ctx->G, R, ctx->K, A,
+    go<NoBatch>(ctx, k_explicit_tma<VAR, real>, grid, XT_THREADS, XtSmem<real, VAR>::DYN, M, ctx->G, R, ctx->K, A,
                                                                                      ctx->status);
     return true;
 }
@@ -108,11 +108,12 @@ void launch_explicit(pllgpu_ctx* ctx, const real* un, const real* vn, const real
         // per block as the tuned shape
         const dim3 blk(EP_DK, bx * by / EP_DK);
         const dim3 grid((nk(R) + 2 * EP_DK - 1) / (2 * EP_DK), (nj(R) + blk.y - 1) / blk.y, ni(R));
-        k_explicit2<VAR><<<grid, blk, 0, ctx->st>>>(ctx->G, R, ctx->K, A);
+        go<k_explicit2_b<VAR>>(ctx, k_explicit2<VAR>, grid, blk, 0, ctx->G, R, ctx->K, A);
     } else {
         if (!ctx->xt_on || ctx->P.explicit_kernel == 1 || !launch_explicit_tma<real, VAR>(ctx, A)) {
             const dim3 blk(bx, by);
-            k_explicit<VAR, real><<<box_grid(nk(R), nj(R), ni(R), blk), blk, 0, ctx->st>>>(ctx->G, R, ctx->K, A);
+            go<k_explicit_b<VAR, real>>(ctx, k_explicit<VAR, real>, box_grid(nk(R), nj(R), ni(R), blk), blk, 0, ctx->G,
+                                        R, ctx->K, A);
         }
     }
     mark(ctx, lab[VAR]);
@@ -130,9 +131,11 @@ void line_seg(pllgpu_ctx* ctx, const Rng& R, const XsweepArgs<real>& X, int n)
     const dim3 grid((nk(R) + 31) / 32, AXIS == 0 ? nj(R) : ni(R)), blk(32 * P);
     constexpr size_t smem = line_seg_smem<VAR, AXIS, P, RS, real>();
     if (n == P * RS)
-        k_line_seg<VAR, AXIS, P, RS, true, real><<<grid, blk, smem, ctx->st>>>(ctx->G, R, ctx->K, X);
+        go<k_line_seg_b<VAR, AXIS, P, RS, true, real>>(ctx, k_line_seg<VAR, AXIS, P, RS, true, real>, grid, blk, smem,
+                                                       ctx->G, R, ctx->K, X);
     else
-        k_line_seg<VAR, AXIS, P, RS, false, real><<<grid, blk, smem, ctx->st>>>(ctx->G, R, ctx->K, X);
+        go<k_line_seg_b<VAR, AXIS, P, RS, false, real>>(ctx, k_line_seg<VAR, AXIS, P, RS, false, real>, grid, blk, smem,
+                                                        ctx->G, R, ctx->K, X);
 }
 
 template <int VAR, int AXIS, typename real>
@@ -219,33 +222,35 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
         // lines
         ydone = launch_line_seg<VAR, 1, real>(ctx, R, X);
         if (!ydone && VAR == VC && nj(R) <= ZP_MAX && nj(R) >= 2 * (ZP_MAX / 32) && !ctx->P.exact_dct) {
-            k_adi_y_part<VAR, float><<<dim3((nk(R) + 31) / 32, ni(R)), 256, adi_y_part_smem<float>(), ctx->st>>>(
-                ctx->G, R, ctx->K, X.mu, B.S, ctx->scal, alpha);
+            go<k_adi_y_part_b<VAR, float>>(ctx, k_adi_y_part<VAR, float>, dim3((nk(R) + 31) / 32, ni(R)), 256,
+                                           adi_y_part_smem<float>(), ctx->G, R, ctx->K, X.mu, B.S, ctx->scal, alpha);
             ydone = true;
         }
     }
     if (!ydone)
-        k_line_pf<VAR, 1, real><<<dim3((nk(R) + lb - 1) / lb, ni(R)), lb, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
+        go<k_line_pf_b<VAR, 1, real>>(ctx, k_line_pf<VAR, 1, real>, dim3((nk(R) + lb - 1) / lb, ni(R)), lb, 0, ctx->G,
+                                      R, ctx->K, X);
     mark(ctx, ly[VAR]);
     bool zdone = false;
     if constexpr (std::is_same<real, float>::value || !PLL_FP64_EXACT) {
         if (nk(R) <= ZP_MAX && nk(R) >= 2 * (ZP_MAX / 32) && !ctx->P.exact_dct) {
             // the partitioned warp solve (precision form and FP64 form)
-            k_adi_z_part<VAR, real><<<dim3((nj(R) + 3) / 4, ni(R)), 128, 0, ctx->st>>>(ctx->G, R, ctx->K, X.mu, B.S,
-                                                                              ctx->scal, alpha);
+            go<k_adi_z_part_b<VAR, real>>(ctx, k_adi_z_part<VAR, real>, dim3((nj(R) + 3) / 4, ni(R)), 128, 0, ctx->G, R,
+                                          ctx->K, X.mu, B.S, ctx->scal, alpha);
             zdone = true;
         }
     }
     if (!zdone) {
         constexpr size_t smem = adi_z_smem_bytes<VAR, real>();
-        k_adi_z_tiled<VAR, real><<<dim3((nj(R) + 127) / 128, ni(R)), 128, smem, ctx->st>>>(
-            ctx->G, R, ctx->K, X.mu, B.S, B.cc, ctx->scal, alpha);
+        go<k_adi_z_tiled_b<VAR, real>>(ctx, k_adi_z_tiled<VAR, real>, dim3((nj(R) + 127) / 128, ni(R)), 128, smem,
+                                       ctx->G, R, ctx->K, X.mu, B.S, B.cc, ctx->scal, alpha);
     }
     mark(ctx, lz[VAR]);
     bool xdone = false;
     if constexpr (std::is_same<real, float>::value) xdone = launch_line_seg<VAR, 0, real>(ctx, R, X);
     if (!xdone)
-        k_line_pf<VAR, 0, real><<<dim3((nk(R) + lb - 1) / lb, nj(R)), lb, 0, ctx->st>>>(ctx->G, R, ctx->K, X);
+        go<k_line_pf_b<VAR, 0, real>>(ctx, k_line_pf<VAR, 0, real>, dim3((nk(R) + lb - 1) / lb, nj(R)), lb, 0, ctx->G,
+                                      R, ctx->K, X);
     mark(ctx, lx[VAR]);
 }
 
@@ -257,16 +262,16 @@ void launch_viscosity(pllgpu_ctx* ctx, const real* cn, MuPtrs<real> m, int law =
         if ((law < 0 ? ctx->P.nmvp : law) == 0) {   // the exponential law on cell pairs
             const dim3 grid((ctx->G.NZ + 2 * EP_DK - 1) / (2 * EP_DK), (ctx->G.NY + blk.y - 1) / blk.y,
                             (ni(ctx->Rg) + 2 + VISC_NI - 1) / VISC_NI);
-            k_viscosity2<real><<<grid, blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->K, cn, (real*)m.cell, (real*)m.xy,
-                                                          (real*)m.xz, (real*)m.yz);
+            go<k_viscosity2_b<real>>(ctx, k_viscosity2<real>, grid, blk, 0, ctx->G, ctx->Rg, ctx->K, cn, (real*)m.cell,
+                                     (real*)m.xy, (real*)m.xz, (real*)m.yz);
             mark(ctx, "viscosity");
             return;
         }
     }
-    k_viscosity<real><<<box_grid(ctx->G.NZ, ctx->G.NY, (ni(ctx->Rg) + 2 + VISC_NI - 1) / VISC_NI, blk), blk, 0,
-                        ctx->st>>>(
-        ctx->G, ctx->Rg, ctx->K, law < 0 ? ctx->P.nmvp : law, cn, (real*)m.cell, (real*)m.xy, (real*)m.xz,
-        (real*)m.yz, ctx->scal);
+    go<k_viscosity_b<real>>(ctx, k_viscosity<real>,
+                            box_grid(ctx->G.NZ, ctx->G.NY, (ni(ctx->Rg) + 2 + VISC_NI - 1) / VISC_NI, blk), blk, 0,
+                            ctx->G, ctx->Rg, ctx->K, law < 0 ? ctx->P.nmvp : law, cn, (real*)m.cell, (real*)m.xy,
+                            (real*)m.xz, (real*)m.yz, ctx->scal);
     mark(ctx, "viscosity");
 }
 
@@ -274,9 +279,9 @@ void launch_gemm(pllgpu_ctx* ctx, const GemmDesc& d, const double* A, const doub
 {
     dim3 grid((d.N + 63) / 64, (d.M + 63) / 64, d.batch);
     if (ctx->P.exact_dct)
-        k_gemm_seq<double><<<grid, 256, 0, ctx->st>>>(d, A, B, C);
+        go<k_gemm_seq_b<double>>(ctx, k_gemm_seq<double>, grid, 256, 0, d, A, B, C);
     else
-        k_gemm_dmma<<<grid, 256, 0, ctx->st>>>(d, A, B, C);
+        go<k_gemm_dmma_b>(ctx, k_gemm_dmma, grid, 256, 0, d, A, B, C);
     mark(ctx, "dct_gemm");
 }
 
@@ -284,9 +289,9 @@ void launch_gemm(pllgpu_ctx* ctx, const GemmDesc& d, const float* A, const float
 {
     dim3 grid((d.N + 63) / 64, (d.M + 63) / 64, d.batch);
     if (ctx->P.exact_dct)
-        k_gemm_seq<float><<<grid, 256, 0, ctx->st>>>(d, A, B, C);
+        go<k_gemm_seq_b<float>>(ctx, k_gemm_seq<float>, grid, 256, 0, d, A, B, C);
     else
-        k_gemm_tf32x3<<<grid, 256, 0, ctx->st>>>(d, A, B, C);
+        go<k_gemm_tf32x3_b>(ctx, k_gemm_tf32x3, grid, 256, 0, d, A, B, C);
     mark(ctx, "dct_gemm");
 }
 
@@ -304,19 +309,19 @@ void launch_umma(pllgpu_ctx* ctx, int pass, long rows, int K, const UmmaEpi& e, 
     if (ctx->P.dct_kernel == 2) {   // one tile per CTA
         const dim3 grid((unsigned)ntiles);
         if (K == 256)
-            k_dct_umma<256><<<grid, UM_THREADS, UmmaSmem<256>::DYN, ctx->st>>>(U.a[pass], U.bh[pass], U.bl[pass],
+            go<NoBatch>(ctx, k_dct_umma<256>, grid, UM_THREADS, UmmaSmem<256>::DYN, U.a[pass], U.bh[pass], U.bl[pass],
                                                                                K, e, out, ctx->status);
         else
-            k_dct_umma<128><<<grid, UM_THREADS, UmmaSmem<128>::DYN, ctx->st>>>(U.a[pass], U.bh[pass], U.bl[pass],
+            go<NoBatch>(ctx, k_dct_umma<128>, grid, UM_THREADS, UmmaSmem<128>::DYN, U.a[pass], U.bh[pass], U.bl[pass],
                                                                                K, e, out, ctx->status);
     } else {   // persistent: one CTA per SM
         const dim3 grid((unsigned)std::min(ntiles, U.sms));
         if (K == 256)
-            k_dct_umma_p<256><<<grid, UMP_THREADS, UmmaPSmem<256>::DYN, ctx->st>>>(
-                U.a[pass], U.bh[pass], U.bl[pass], K, ntiles, e, out, ctx->status);
+            go<NoBatch>(ctx, k_dct_umma_p<256>, grid, UMP_THREADS, UmmaPSmem<256>::DYN, U.a[pass], U.bh[pass],
+                        U.bl[pass], K, ntiles, e, out, ctx->status);
         else
-            k_dct_umma_p<128><<<grid, UMP_THREADS, UmmaPSmem<128>::DYN, ctx->st>>>(
-                U.a[pass], U.bh[pass], U.bl[pass], K, ntiles, e, out, ctx->status);
+            go<NoBatch>(ctx, k_dct_umma_p<128>, grid, UMP_THREADS, UmmaPSmem<128>::DYN, U.a[pass], U.bh[pass],
+                        U.bl[pass], K, ntiles, e, out, ctx->status);
     }
     mark(ctx, "dct_umma");
 }
@@ -330,8 +335,8 @@ void launch_poisson_umma(pllgpu_ctx* ctx)
     launch_umma(ctx, 0, (long)nx * ny, nz, UmmaEpi{ny, N, 1, ny, 1.f, 0, 1}, B.dct2);
     // forward y: dct1[x][kz][ky] = sum_y dct2[x][kz][y] Ty[ky][y]
     launch_umma(ctx, 1, (long)nx * nz, ny, UmmaEpi{nz, N, ny, 1, 1.f, 0, 0}, B.dct1);
-    k_poisson_x2<<<(int)((N + 127) / 128), 128, 0, ctx->st>>>(nx, ny, nz, ctx->K, ctx->lam_y, ctx->lam_z, B.dct1,
-                                                             (float*)ctx->mode_rr, ctx->mode_cc, 1);
+    go<k_poisson_x2_b>(ctx, k_poisson_x2, (int)((N + 127) / 128), 128, 0, nx, ny, nz, ctx->K, ctx->lam_y, ctx->lam_z,
+                       B.dct1, (float*)ctx->mode_rr, ctx->mode_cc, 1);
     mark(ctx, "poisson_x");
     // inverse y: dct2[x][y][kz] = sum_ky dct1[x][kz][ky] Tiy[y][ky] (stored transposed)
     launch_umma(ctx, 2, (long)nx * nz, ny, UmmaEpi{nz, N, 1, nz, 1.f, 0, 1}, B.dct2);
@@ -351,8 +356,8 @@ template <int N, int KIND, bool CONTIG>
 void fft_launch(pllgpu_ctx* ctx, const FftLines& d, int axis, const double* in, double* out)
 {
     const unsigned grid = (unsigned)(d.lines / (2 * FFT_PB));
-    k_dct_fft<double, N, KIND, CONTIG><<<grid, FFT_THREADS, fft_smem_bytes<N>(), ctx->st>>>(
-        d, in, out, ctx->fft_tw[axis], ctx->fft_wq[axis]);
+    go<k_dct_fft_b<double, N, KIND, CONTIG>>(ctx, k_dct_fft<double, N, KIND, CONTIG>, grid, FFT_THREADS,
+                                             fft_smem_bytes<N>(), d, in, out, ctx->fft_tw[axis], ctx->fft_wq[axis]);
 }
 
 template <int KIND, bool CONTIG>
@@ -379,8 +384,8 @@ void launch_poisson_fft(pllgpu_ctx* ctx)
     const FftLines zlines{nx * ny, ny, N, nz, 1, N, nz, 1, 1.0};
     fft_pass<0, false>(ctx, ny, ylines, 0, B.dct1, B.dct2);
     fft_pass<0, true>(ctx, nz, zlines, 1, B.dct2, B.dct1);
-    k_poisson_x<double><<<(int)((N + 127) / 128), 128, 0, ctx->st>>>(nx, ny, nz, ctx->K, ctx->lam_y, ctx->lam_z,
-                                                                    B.dct1, ctx->mode_cc, ctx->mode_rr);
+    go<k_poisson_x_b<double>>(ctx, k_poisson_x<double>, (int)((N + 127) / 128), 128, 0, nx, ny, nz, ctx->K,
+                              ctx->lam_y, ctx->lam_z, B.dct1, ctx->mode_cc, ctx->mode_rr, 0);
     mark(ctx, "poisson_x");
     fft_pass<1, false>(ctx, ny, ylines, 0, B.dct1, B.dct2);
     // into phi's interior, times 1/(4 ny nz) (exact: a power of two)
@@ -421,8 +426,8 @@ void launch_poisson(pllgpu_ctx* ctx)
     d = GemmDesc{ny, nz, nz, nx, N, nz, 1, 0, 1, nz, N, nz, 1, 0.0, 0};
     launch_gemm(ctx, d, B.dct2, B.Tz, B.dct1);
     // x-tridiagonal per mode, in place in dct1, FP64 arithmetic
-    k_poisson_x<real><<<(int)((N + 127) / 128), 128, 0, ctx->st>>>(nx, ny, nz, ctx->K, ctx->lam_y, ctx->lam_z,
-                                                                  B.dct1, ctx->mode_cc, ctx->mode_rr);
+    go<k_poisson_x_b<real>>(ctx, k_poisson_x<real>, (int)((N + 127) / 128), 128, 0, nx, ny, nz, ctx->K,
+                            ctx->lam_y, ctx->lam_z, B.dct1, ctx->mode_cc, ctx->mode_rr, 0);
     mark(ctx, "poisson_x");
     // inverse, y pass: dct2[x][y][kz] = sum_ky Tiy[y][ky] dct1[x][ky][kz]
     d = GemmDesc{ny, nz, ny, nx, 0, ny, 1, N, nz, 1, N, nz, 1, 0.0, 0};
@@ -440,11 +445,11 @@ void launch_phi_ghosts(pllgpu_ctx* ctx)
 {
     const Rng& R = ctx->Rg;
     real* phi = bufs<real>(ctx).phi;
-    k_phi_ghosts<0, real><<<dim3((nj(R) + 127) / 128, ni(R)), 128, 0, ctx->st>>>(ctx->G, R, phi);
+    go<k_phi_ghosts_b<0, real>>(ctx, k_phi_ghosts<0, real>, dim3((nj(R) + 127) / 128, ni(R)), 128, 0, ctx->G, R, phi);
     mark(ctx, "phi_ghosts");
-    k_phi_ghosts<1, real><<<dim3((nk(R) + 127) / 128, ni(R)), 128, 0, ctx->st>>>(ctx->G, R, phi);
+    go<k_phi_ghosts_b<1, real>>(ctx, k_phi_ghosts<1, real>, dim3((nk(R) + 127) / 128, ni(R)), 128, 0, ctx->G, R, phi);
     mark(ctx, "phi_ghosts");
-    k_phi_ghosts<2, real><<<dim3((nk(R) + 127) / 128, nj(R)), 128, 0, ctx->st>>>(ctx->G, R, phi);
+    go<k_phi_ghosts_b<2, real>>(ctx, k_phi_ghosts<2, real>, dim3((nk(R) + 127) / 128, nj(R)), 128, 0, ctx->G, R, phi);
     mark(ctx, "phi_ghosts");
 }
 
@@ -457,18 +462,17 @@ void launch_project(pllgpu_ctx* ctx, double alpha, int correct, int ghosts, int 
     if constexpr (std::is_same<real, float>::value || !PLL_FP64_EXACT) {
         const dim3 grid((nk(ctx->Rg) + 2 * EP_DK - 1) / (2 * EP_DK), (nj(ctx->Rg) + blk.y - 1) / blk.y,
                         ni(ctx->Rg) + 1);
-        k_project2<real><<<grid, blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->Rv[VU], ctx->Rv[VV], ctx->Rv[VW], ctx->K,
-                                              q_new<real>(ctx, VU), q_new<real>(ctx, VV), q_new<real>(ctx, VW),
-                                              B.pg[VU], B.pg[VV], B.pg[VW], B.phi, mu, ctx->scal, alpha, correct,
-                                              ghosts, pgu);
+        go<k_project2_b<real>>(ctx, k_project2<real>, grid, blk, 0, ctx->G, ctx->Rg, ctx->Rv[VU], ctx->Rv[VV],
+                               ctx->Rv[VW], ctx->K, q_new<real>(ctx, VU), q_new<real>(ctx, VV), q_new<real>(ctx, VW),
+                               B.pg[VU], B.pg[VV], B.pg[VW], B.phi, mu, ctx->scal, alpha, correct, ghosts, pgu);
         mark(ctx, "project");
         return;
     }
-    k_project<real><<<box_grid(nk(ctx->Rg), nj(ctx->Rg), (ni(ctx->Rg) + 1 + PROJECT_NI - 1) / PROJECT_NI, blk),
-                      blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->Rv[VU], ctx->Rv[VV], ctx->Rv[VW], ctx->K,
-                                         q_new<real>(ctx, VU), q_new<real>(ctx, VV), q_new<real>(ctx, VW),
-                                         B.pg[VU], B.pg[VV], B.pg[VW], B.phi, mu.cell, mu.xy, mu.xz, mu.yz,
-                                         ctx->scal, alpha, correct, ghosts, pgu);
+    go<k_project_b<real>>(ctx, k_project<real>,
+                          box_grid(nk(ctx->Rg), nj(ctx->Rg), (ni(ctx->Rg) + 1 + PROJECT_NI - 1) / PROJECT_NI, blk), blk,
+                          0, ctx->G, ctx->Rg, ctx->Rv[VU], ctx->Rv[VV], ctx->Rv[VW], ctx->K, q_new<real>(ctx, VU),
+                          q_new<real>(ctx, VV), q_new<real>(ctx, VW), B.pg[VU], B.pg[VV], B.pg[VW], B.phi, mu.cell,
+                          mu.xy, mu.xz, mu.yz, ctx->scal, alpha, correct, ghosts, pgu);
     mark(ctx, "project");
 }
 
@@ -481,15 +485,15 @@ void launch_div(pllgpu_ctx* ctx, int mode, double alpha)
         if (mode == 0) {   // the right-hand side on cell pairs
             const dim3 grid((nk(ctx->Rg) + 2 * EP_DK - 1) / (2 * EP_DK), (nj(ctx->Rg) + blk.y - 1) / blk.y,
                             (ni(ctx->Rg) + DIV_NI - 1) / DIV_NI);
-            k_div_rhs2<real><<<grid, blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->K, q_new<real>(ctx, VU), q_new<real>(ctx, VV),
-                                                  q_new<real>(ctx, VW), B.dct1, ctx->scal, alpha);
+            go<k_div_rhs2_b<real>>(ctx, k_div_rhs2<real>, grid, blk, 0, ctx->G, ctx->Rg, ctx->K, q_new<real>(ctx, VU),
+                                   q_new<real>(ctx, VV), q_new<real>(ctx, VW), B.dct1, ctx->scal, alpha);
             mark(ctx, "div_rhs");
             return;
         }
     }
-    k_div_rhs<real><<<box_grid(nk(ctx->Rg), nj(ctx->Rg), ni(ctx->Rg), blk), blk, 0, ctx->st>>>(
-        ctx->G, ctx->Rg, ctx->K, q_new<real>(ctx, VU), q_new<real>(ctx, VV), q_new<real>(ctx, VW), B.div, B.div,
-        B.dct1, ctx->scal, alpha, mode);
+    go<k_div_rhs_b<real>>(ctx, k_div_rhs<real>, box_grid(nk(ctx->Rg), nj(ctx->Rg), ni(ctx->Rg), blk), blk, 0, ctx->G,
+                          ctx->Rg, ctx->K, q_new<real>(ctx, VU), q_new<real>(ctx, VV), q_new<real>(ctx, VW), B.div,
+                          B.div, B.dct1, ctx->scal, alpha, mode);
     mark(ctx, "div_rhs");
 }
 
@@ -498,12 +502,12 @@ void launch_flux(pllgpu_ctx* ctx)
 {
     if constexpr (std::is_same<real, float>::value) {
         const int rows = 2 * nj(ctx->Rv[VU]);
-        k_flux3<<<(rows + 31) / 32, 1024, 0, ctx->st>>>(ctx->G, ctx->Rv[VU], ctx->K, q_new<real>(ctx, VU), ctx->red,
-                                                        ctx->ticket, ctx->scal);
+        go<k_flux3_b>(ctx, k_flux3, (rows + 31) / 32, 1024, 0, ctx->G, ctx->Rv[VU], ctx->K, q_new<real>(ctx, VU),
+                      ctx->red, ctx->ticket, ctx->scal);
         mark(ctx, "flux");
         return;
     }
-    k_flux<real><<<1, 512, sizeof(double) * 2 * ctx->G.NY, ctx->st>>>(ctx->G, ctx->Rv[VU], ctx->K,
+    go<k_flux_b<real>>(ctx, k_flux<real>, 1, 512, sizeof(double) * 2 * ctx->G.NY, ctx->G, ctx->Rv[VU], ctx->K,
                                                                        q_new<real>(ctx, VU), ctx->scal);
     mark(ctx, "flux");
 }
@@ -511,7 +515,7 @@ void launch_flux(pllgpu_ctx* ctx)
 template <typename real>
 void launch_bulk(pllgpu_ctx* ctx)
 {
-    k_bulk2<real><<<BULK_BLOCKS, 1024, 0, ctx->st>>>(ctx->G, ctx->Rg, q_old<real>(ctx, VU), ctx->red,
+    go<k_bulk2_b<real>>(ctx, k_bulk2<real>, BULK_BLOCKS, 1024, 0, ctx->G, ctx->Rg, q_old<real>(ctx, VU), ctx->red,
                                                       ctx->ticket + 1, ctx->scal);
     mark(ctx, "bulk_velo");
 }
@@ -523,15 +527,15 @@ void launch_cfl(pllgpu_ctx* ctx)
     if constexpr (std::is_same<real, float>::value) {
         const dim3 grid((nk(ctx->Rg) + 2 * EP_DK - 1) / (2 * EP_DK), (nj(ctx->Rg) + blk.y - 1) / blk.y,
                         (ni(ctx->Rg) + CFL_NI - 1) / CFL_NI);
-        k_cfl2<<<grid, blk, 0, ctx->st>>>(ctx->G, ctx->Rg, ctx->K, q_old<real>(ctx, VU), q_old<real>(ctx, VV),
+        go<k_cfl2_b>(ctx, k_cfl2, grid, blk, 0, ctx->G, ctx->Rg, ctx->K, q_old<real>(ctx, VU), q_old<real>(ctx, VV),
                                           q_old<real>(ctx, VW), ctx->scal, ctx->status);
     } else {
-        k_cfl<real><<<box_grid(nk(ctx->Rg), nj(ctx->Rg), ni(ctx->Rg), blk), blk, 0, ctx->st>>>(
-            ctx->G, ctx->Rg, ctx->K, q_old<real>(ctx, VU), q_old<real>(ctx, VV), q_old<real>(ctx, VW), ctx->scal,
-            ctx->status);
+        go<k_cfl_b<real>>(ctx, k_cfl<real>, box_grid(nk(ctx->Rg), nj(ctx->Rg), ni(ctx->Rg), blk), blk, 0, ctx->G,
+                          ctx->Rg, ctx->K, q_old<real>(ctx, VU), q_old<real>(ctx, VV), q_old<real>(ctx, VW), ctx->scal,
+                          ctx->status);
     }
     mark(ctx, "cfl");
-    k_dt<<<1, 1, 0, ctx->st>>>(ctx->K, ctx->scal);
+    go<k_dt_b>(ctx, k_dt, 1, 1, 0, ctx->K, ctx->scal);
     mark(ctx, "dt");
 }
 
@@ -572,7 +576,7 @@ void enqueue_substep(pllgpu_ctx* ctx, int rk)
     }
 }
 
-__global__ void k_tval(double* scal, double a0, double a1, double a2)
+__device__ __forceinline__ void k_tval_run(const uint3, const dim3, double* scal, double a0, double a1, double a2)
 {
     // tval += (gamma+rho) dt per substep, pllcart3d.c:166
     const double dt = scal[S_DT];
@@ -582,13 +586,21 @@ __global__ void k_tval(double* scal, double a0, double a1, double a2)
     t = t + a2 * dt;
     scal[S_TVAL] = t;
 }
+__global__ void k_tval(double* scal, double a0, double a1, double a2)
+{
+    k_tval_run(blockIdx, gridDim, scal, a0, a1, a2);
+}
+struct k_tval_b {
+    static constexpr auto run = &k_tval_run;
+    static constexpr int maxt = 0, minb = 0;
+};
 
 template <typename real>
 void enqueue_step(pllgpu_ctx* ctx)
 {
     launch_cfl<real>(ctx);
     for (int rk = 0; rk < 3; ++rk) enqueue_substep<real>(ctx, rk);
-    k_tval<<<1, 1, 0, ctx->st>>>(ctx->scal, kRK1[0] + kRK2[0], kRK1[1] + kRK2[1], kRK1[2] + kRK2[2]);
+    go<k_tval_b>(ctx, k_tval, 1, 1, 0, ctx->scal, kRK1[0] + kRK2[0], kRK1[1] + kRK2[1], kRK1[2] + kRK2[2]);
     mark(ctx, "tval");
 }
 

@@ -52,6 +52,35 @@ __device__ __forceinline__ float over_2h<float>(float x, double, double i2h, int
     return x * (float)i2h;
 }
 
+// g a + r b, the RK combination of the explicit terms.  The exact form
+// rounds both products and the sum as the reference does (it is compiled
+// without contraction); the other forms fuse the first product and round
+// the second on its own, so that the result does not depend on which of the
+// two products a compiler would have fused.
+__device__ __forceinline__ float mul_rn_(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn_(double a, double b) { return __dmul_rn(a, b); }
+template <typename real>
+__device__ __forceinline__ real rk_comb(real g, real a, real r, real b)
+{
+#if PLL_FP64_EXACT
+    if (sizeof(real) == 8) return g * a + r * b;
+#endif
+    return fma(g, a, mul_rn_(r, b));
+}
+
+// dt (g a + r b), the convective outflow increment of an x sweep: a rounded
+// product outside the exact form, since it feeds both q_new = q_old + it and
+// the last row's right-hand side (a product with two uses, which a compiler
+// may fuse into either)
+template <typename real>
+__device__ __forceinline__ real rk_step(real dt, real g, real a, real r, real b)
+{
+#if PLL_FP64_EXACT
+    if (sizeof(real) == 8) return dt * (g * a + r * b);
+#endif
+    return mul_rn_(dt, rk_comb<real>(g, a, r, b));
+}
+
 // advecting velocity of variable VAR for the pass along AXIS at point id
 // (Hc_op L1563/1591/1621, Hu_op L1669/1696/1722, Hv_op L1780/1807/1834,
 //  Hw_op L1892/1919/1946)
@@ -368,7 +397,8 @@ struct ExplicitArgs {
 // L1280-1298)
 // ---------------------------------------------------------------------------
 template <int VAR, typename real>
-__global__ void __launch_bounds__(128) k_explicit(Geo G, Rng R, Consts K,
+__device__ __forceinline__ void k_explicit_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng R, Consts K,
                                                   ExplicitArgs<real> A)
 {
     const int k = R.ks + blockIdx.x * blockDim.x + threadIdx.x;
@@ -417,7 +447,7 @@ __global__ void __launch_bounds__(128) k_explicit(Geo G, Rng R, Consts K,
     // right-hand side dt*(gamma H + rho H_old + alpha A q_old + alpha body)
     const real dt = (real)A.scal[S_DT];
     const real alpha = (real)A.alpha;
-    real conv = ((real)A.g * H + (real)A.r * A.Hm[id]);
+    real conv = rk_comb<real>((real)A.g, H, (real)A.r, A.Hm[id]);
     real a, b, c;
     acoef<VAR, 0, real>(K, G, A.mu.cell, A.mu.xy, A.mu.xz, A.mu.yz, id, a, b, c);
     real ax = a * q[id - sx] + b * q[id] + c * q[id + sx];
@@ -444,6 +474,17 @@ __global__ void __launch_bounds__(128) k_explicit(Geo G, Rng R, Consts K,
     }
     A.S[id] = S;
 }
+template <int VAR, typename real>
+__global__ void __launch_bounds__(128) k_explicit(Geo G, Rng R, Consts K,
+                                                  ExplicitArgs<real> A)
+{
+    k_explicit_run<VAR, real>(blockIdx, gridDim, G, R, K, A);
+}
+template <int VAR, typename real>
+struct k_explicit_b {
+    static constexpr auto run = &k_explicit_run<VAR, real>;
+    static constexpr int maxt = 128, minb = 0;
+};
 
 // ---------------------------------------------------------------------------
 // The precision form's explicit operator on cell pairs with packed FP32x2
@@ -633,7 +674,8 @@ __device__ __forceinline__ void acoef2(const Consts& K, const Geo& G, const MuPt
 
 // grid: x over k in tiles of 2 * EP_DK (blockDim.x == EP_DK), y over j, z over i
 template <int VAR>
-__global__ void __launch_bounds__(128, 16) k_explicit2(Geo G, Rng R, Consts K, ExplicitArgs<float> A)
+__device__ __forceinline__ void k_explicit2_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng R, Consts K, ExplicitArgs<float> A)
 {
     const int k = R.ks + blockIdx.x * (2 * EP_DK) + threadIdx.x;
     const int j = R.js + blockIdx.y * blockDim.y + threadIdx.y;
@@ -713,6 +755,16 @@ __global__ void __launch_bounds__(128, 16) k_explicit2(Geo G, Rng R, Consts K, E
     A.S[id] = S.v.x;
     if (live_b) A.S[id + EP_DK] = S.v.y;
 }
+template <int VAR>
+__global__ void __launch_bounds__(128, 16) k_explicit2(Geo G, Rng R, Consts K, ExplicitArgs<float> A)
+{
+    k_explicit2_run<VAR>(blockIdx, gridDim, G, R, K, A);
+}
+template <int VAR>
+struct k_explicit2_b {
+    static constexpr auto run = &k_explicit2_run<VAR>;
+    static constexpr int maxt = 128, minb = 16, bminb = 8;
+};
 
 // closure codes of the first/last unknown of an ADI line:
 // 1 b+=a (Neumann / symmetry), 2 b-=a (reflection about a wall face),
@@ -762,7 +814,8 @@ constexpr size_t adi_z_smem_bytes()
 }
 
 template <int VAR, typename real>
-__global__ void __launch_bounds__(128, 4) k_adi_z_tiled(Geo G, Rng R, Consts K, MuPtrs<real> mu,
+__device__ __forceinline__ void k_adi_z_tiled_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng R, Consts K, MuPtrs<real> mu,
                                                      real* __restrict__ S, real* __restrict__ cc,
                                                      const double* __restrict__ scal, double alpha)
 {
@@ -918,6 +971,18 @@ __global__ void __launch_bounds__(128, 4) k_adi_z_tiled(Geo G, Rng R, Consts K, 
         __syncwarp();
     }
 }
+template <int VAR, typename real>
+__global__ void __launch_bounds__(128, 4) k_adi_z_tiled(Geo G, Rng R, Consts K, MuPtrs<real> mu,
+                                                     real* __restrict__ S, real* __restrict__ cc,
+                                                     const double* __restrict__ scal, double alpha)
+{
+    k_adi_z_tiled_run<VAR, real>(blockIdx, gridDim, G, R, K, mu, S, cc, scal, alpha);
+}
+template <int VAR, typename real>
+struct k_adi_z_tiled_b {
+    static constexpr auto run = &k_adi_z_tiled_run<VAR, real>;
+    static constexpr int maxt = 128, minb = 4;
+};
 
 
 // ---------------------------------------------------------------------------
@@ -1025,7 +1090,8 @@ __device__ __forceinline__ void zp_solve(const real* A, const real* B, const rea
 }
 
 template <int VAR, typename real>
-__global__ void __launch_bounds__(128) k_adi_z_part(Geo G, Rng R, Consts K, MuPtrs<real> mu,
+__device__ __forceinline__ void k_adi_z_part_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng R, Consts K, MuPtrs<real> mu,
                                                     real* __restrict__ S, const double* __restrict__ scal,
                                                     double alpha)
 {
@@ -1105,6 +1171,18 @@ __global__ void __launch_bounds__(128) k_adi_z_part(Geo G, Rng R, Consts K, MuPt
         if (m < n) S[base + m] = sS[zp_skew(m)];
     }
 }
+template <int VAR, typename real>
+__global__ void __launch_bounds__(128) k_adi_z_part(Geo G, Rng R, Consts K, MuPtrs<real> mu,
+                                                    real* __restrict__ S, const double* __restrict__ scal,
+                                                    double alpha)
+{
+    k_adi_z_part_run<VAR, real>(blockIdx, gridDim, G, R, K, mu, S, scal, alpha);
+}
+template <int VAR, typename real>
+struct k_adi_z_part_b {
+    static constexpr auto run = &k_adi_z_part_run<VAR, real>;
+    static constexpr int maxt = 128, minb = 0;
+};
 
 
 // ---------------------------------------------------------------------------
@@ -1161,7 +1239,8 @@ template <typename real>
 constexpr size_t adi_y_part_smem() { return sizeof(real) * 2 * 32 * YP_PITCH; }
 
 template <int VAR, typename real>
-__global__ void __launch_bounds__(256) k_adi_y_part(Geo G, Rng R, Consts K, MuPtrs<real> mu,
+__device__ __forceinline__ void k_adi_y_part_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng R, Consts K, MuPtrs<real> mu,
                                                     real* __restrict__ S, const double* __restrict__ scal,
                                                     double alpha)
 {
@@ -1247,6 +1326,18 @@ __global__ void __launch_bounds__(256) k_adi_y_part(Geo G, Rng R, Consts K, MuPt
         if (tkl < nl && m < n) S[base0 + (long)m * sy + tkl] = tS[tkl * YP_PITCH + zp_skew(m)];
     }
 }
+template <int VAR, typename real>
+__global__ void __launch_bounds__(256) k_adi_y_part(Geo G, Rng R, Consts K, MuPtrs<real> mu,
+                                                    real* __restrict__ S, const double* __restrict__ scal,
+                                                    double alpha)
+{
+    k_adi_y_part_run<VAR, real>(blockIdx, gridDim, G, R, K, mu, S, scal, alpha);
+}
+template <int VAR, typename real>
+struct k_adi_y_part_b {
+    static constexpr auto run = &k_adi_y_part_run<VAR, real>;
+    static constexpr int maxt = 256, minb = 0;
+};
 
 // ---------------------------------------------------------------------------
 // Line solves along a strided axis (AXIS 0: x, lines (j,k); AXIS 1: y,
@@ -1260,7 +1351,8 @@ __global__ void __launch_bounds__(256) k_adi_y_part(Geo G, Rng R, Consts K, MuPt
 // and, for c, the Neumann ghosts of pllcart3d.c:700-712.
 // ---------------------------------------------------------------------------
 template <int VAR, int AXIS, typename real>
-__global__ void __launch_bounds__(128) k_line_pf(Geo G, Rng R, Consts K, XsweepArgs<real> A)
+__device__ __forceinline__ void k_line_pf_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng R, Consts K, XsweepArgs<real> A)
 {
     constexpr int PF = 8;
     const int k = R.ks + blockIdx.x * blockDim.x + threadIdx.x;
@@ -1284,7 +1376,7 @@ __global__ void __launch_bounds__(128) k_line_pf(Geo G, Rng R, Consts K, XsweepA
         real Hb = -(real)A.scal[S_VBULK] * (A.q[rb] - A.q[rb - st]);
         Hb = over_h<real>(Hb, K.hx, K.ihx, K.pow2);
         A.H[rb] = Hb;
-        boun = dt * ((real)A.g * Hb + (real)A.r * A.Hm[rb]);
+        boun = rk_step<real>(dt, (real)A.g, Hb, (real)A.r, A.Hm[rb]);
         A.qn[rb] = A.q[rb] + boun;
     }
 
@@ -1430,6 +1522,16 @@ __global__ void __launch_bounds__(128) k_line_pf(Geo G, Rng R, Consts K, XsweepA
     }
 
 }
+template <int VAR, int AXIS, typename real>
+__global__ void __launch_bounds__(128) k_line_pf(Geo G, Rng R, Consts K, XsweepArgs<real> A)
+{
+    k_line_pf_run<VAR, AXIS, real>(blockIdx, gridDim, G, R, K, A);
+}
+template <int VAR, int AXIS, typename real>
+struct k_line_pf_b {
+    static constexpr auto run = &k_line_pf_run<VAR, AXIS, real>;
+    static constexpr int maxt = 128, minb = 0;
+};
 
 // ---------------------------------------------------------------------------
 // The precision form's line solve along a strided axis (x or y) by a
@@ -1483,8 +1585,8 @@ __device__ __forceinline__ void ls_fresh(double& x) { asm volatile("" : "+d"(x))
 // segment's last row is an identity row (its loads read the row past the
 // line, which the host checks lies inside the padded box)
 template <int VAR, int AXIS, int P, int RS, bool FULL, typename real = float>
-__global__ void __launch_bounds__(32 * P, (RS <= 16 && sizeof(real) == 4) ? 2 : 1)
-    k_line_seg(Geo G, Rng R, Consts K, XsweepArgs<real> A)
+__device__ __forceinline__ void k_line_seg_run(const uint3 blockIdx, const dim3 gridDim,
+    Geo G, Rng R, Consts K, XsweepArgs<real> A)
 {
     __shared__ real eq[4][P][32];       // separator equations
     __shared__ real tail[3][P][32];     // last interior row of each segment
@@ -1543,7 +1645,7 @@ __global__ void __launch_bounds__(32 * P, (RS <= 16 && sizeof(real) == 4) ? 2 : 
         real Hb = -(real)A.scal[S_VBULK] * (A.q[rb] - A.q[rb - st]);
         Hb = over_h<real>(Hb, K.hx, K.ihx, K.pow2);
         A.H[rb] = Hb;
-        boun = dt * ((real)A.g * Hb + (real)A.r * A.Hm[rb]);
+        boun = rk_step<real>(dt, (real)A.g, Hb, (real)A.r, A.Hm[rb]);
         A.qn[rb] = A.q[rb] + boun;
     }
     if (VAR != VC) {
@@ -1737,6 +1839,17 @@ __global__ void __launch_bounds__(32 * P, (RS <= 16 && sizeof(real) == 4) ? 2 : 
     }
     put(0, Sl);
 }
+template <int VAR, int AXIS, int P, int RS, bool FULL, typename real = float>
+__global__ void __launch_bounds__(32 * P, (RS <= 16 && sizeof(real) == 4) ? 2 : 1)
+    k_line_seg(Geo G, Rng R, Consts K, XsweepArgs<real> A)
+{
+    k_line_seg_run<VAR, AXIS, P, RS, FULL, real>(blockIdx, gridDim, G, R, K, A);
+}
+template <int VAR, int AXIS, int P, int RS, bool FULL, typename real = float>
+struct k_line_seg_b {
+    static constexpr auto run = &k_line_seg_run<VAR, AXIS, P, RS, FULL, real>;
+    static constexpr int maxt = 32 * P, minb = (RS <= 16 && sizeof(real) == 4) ? 2 : 1;
+};
 
 }  // namespace
 }  // namespace pll

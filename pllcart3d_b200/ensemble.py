@@ -2,8 +2,10 @@
 
 ``Ensemble`` wraps the ``pllgpu_ensemble_*`` C ABI: every member is an
 ordinary context (``Ensemble.members[i]`` is a :class:`Solver` view of it)
-and one CUDA graph launch advances every member by one step, the members'
-kernels sharing the SMs.  ``random_members`` draws the members of the
+and one CUDA graph launch advances every member by one step.  Members of one
+grid form a class that issues one launch per stage for all of its members
+(``set_batching(False)``: one graph branch per member instead).
+``random_members`` draws the members of the
 ensemble workload: grids from {32^3, 64x32x32, 64^3, 128x64x64}, R ~ U[0,3],
 Pe log-uniform in [500, 5000], Re ~ U[100, 1000], the 64x32x32 workload's
 interface recipe with a per-member seed.
@@ -13,7 +15,8 @@ interface recipe with a per-member seed.
 
 prints one JSON line: aggregate cell-steps/s of the ensemble graph against
 the same members run one after another (each alone, graph-stepped), with
-every member's result checked equal between the two.  With --snapshots,
+every member's result checked equal between the two, and (--branches) the
+rate of the graph with one branch per member.  With --snapshots,
 every 8th step's (c, u, v, w) interior of every member goes to DIR as
 ``member%03d.npz`` (the surrogate's training data).
 """
@@ -105,6 +108,21 @@ class Ensemble:
     def launches_per_step(self) -> int:
         return self._L.pllgpu_ensemble_launches_per_step(self._h)
 
+    @property
+    def classes(self) -> int:
+        """Branches (classes of members with the same launches, or groups of
+        a class) of the graphs last built."""
+        return self._L.pllgpu_ensemble_classes(self._h)
+
+    def set_batching(self, mode) -> int:
+        """1 / True (the default): one launch per stage and class; k >= 2:
+        classes split into groups of at most k members; 0 / False: every
+        member's own launches as its own branch.  Returns the previous mode."""
+        old = self._L.pllgpu_ensemble_set_batching(self._h, int(mode))
+        if old < 0:
+            raise _lib.PllGpuError(-old, "ensemble_set_batching")
+        return old
+
     def cells(self) -> int:
         return sum(w.params.nx * w.params.ny * w.params.nz for w in self.workloads)
 
@@ -134,6 +152,10 @@ def main(argv=None) -> int:
     ap.add_argument("--snapshots", default=None)
     ap.add_argument("--every", type=int, default=8)
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--branches", type=int, default=100,
+                    help="also time this many steps of the graph with one branch per member (0: skip)")
+    ap.add_argument("--group", type=int, default=1,
+                    help="members per batched launch at most (1: whole classes)")
     args = ap.parse_args(argv)
     import torch
 
@@ -141,9 +163,23 @@ def main(argv=None) -> int:
     ens = Ensemble(wls, precision=args.precision)
     ens.load_ics()
     tuned_steps = 0 if args.no_tune else ens.autotune(1)
+    done = tuned_steps
+    branch = None
+    if args.branches > 0:
+        # every member's own launches, one graph branch per member
+        ens.set_batching(False)
+        ens.step(2)   # warm-up, graph capture
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ens.step(args.branches)
+        torch.cuda.synchronize()
+        branch = {"cell_steps_per_s": ens.cells() * args.branches / (time.perf_counter() - t0),
+                  "launches_per_graph_step": ens.launches_per_step, "steps": args.branches}
+        done += 2 + args.branches
+    ens.set_batching(args.group)
     ens.step(2)   # warm-up, graph capture
     torch.cuda.synchronize()
-    done = tuned_steps + 2
+    done += 2
     snaps = {i: [] for i in range(len(wls))} if args.snapshots else None
     t0 = time.perf_counter()
     timed = 0
@@ -189,7 +225,8 @@ def main(argv=None) -> int:
         "precision": args.precision, "steps": done, "timed_steps": timed,
         "cells": ens.cells(), "ensemble_cell_steps_per_s": ens_cells,
         "sequential_cell_steps_per_s": seq_cells, "speedup": ens_cells / seq_cells,
-        "launches_per_graph_step": ens.launches_per_step, "autotune_steps": tuned_steps,
+        "launches_per_graph_step": ens.launches_per_step, "branches": ens.classes, "group": args.group,
+        "one_branch_per_member": branch, "autotune_steps": tuned_steps,
         "members_equal_to_single_runs": mismatches == 0,
         "grids": [list(w.params.shape) for w in wls]}
     print(json.dumps(rep))

@@ -56,6 +56,55 @@ def test_members_equal_single_runs(precision):
     ens.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed64", "mixed"])
+def test_batched_classes_equal_single_runs(precision):
+    """Members sharing a grid form a class that issues one launch per stage
+    (a kernel body over all of the class's members): every member still
+    equals its own single run bit for bit, and the batched graph issues
+    fewer launches than one branch per member."""
+    from pllcart3d_b200.ensemble import Ensemble
+
+    specs = [((16, 8, 8), 2.0, 1000.0, 100.0), ((24, 12, 12), 0.5, 700.0, 400.0),
+             ((16, 8, 8), 0.7, 2500.0, 800.0), ((24, 12, 12), 2.6, 900.0, 150.0),
+             ((16, 8, 8), 1.4, 600.0, 300.0), ((32, 16, 16), 2.9, 3000.0, 900.0)]
+    classes = 3
+    if precision == "mixed":
+        # a class whose DCT passes (tcgen05, tensor-map arguments) replay
+        # per member inside the batched branch
+        specs += [((8, 128, 128), 1.5, 2000.0, 500.0), ((8, 128, 128), 0.4, 1200.0, 200.0)]
+        classes = 4
+    wls = _members(specs)
+    ens = Ensemble(wls, precision=precision)
+    ens.load_ics()
+    ens.step(3)
+    assert ens.classes == classes
+    batched = ens.launches_per_step
+    ens.step(4)
+    for m, w in zip(ens.members, wls):
+        s = _single(w, precision, 7)
+        for f in FIELDS:
+            assert np.array_equal(m.get(f), s.get(f)), (w.name, f)
+        assert m.tval == s.tval
+    # one branch per member: same results, more launches
+    assert ens.set_batching(False)
+    ens.step(2)
+    assert ens.classes == len(wls)
+    assert ens.launches_per_step > batched
+    for m, w in zip(ens.members, wls):
+        s = _single(w, precision, 9)
+        assert np.array_equal(m.get("c_new"), s.get("c_new")), w.name
+    # classes split into groups of at most 2 members, one branch each
+    assert ens.set_batching(2) == 0
+    ens.step(2)
+    assert ens.classes == classes + 1   # the 3-member class makes 2 groups
+    assert batched < ens.launches_per_step
+    for m, w in zip(ens.members, wls):
+        s = _single(w, precision, 11)
+        for f in FIELDS:
+            assert np.array_equal(m.get(f), s.get(f)), (w.name, f)
+    ens.close()
+
+
 def test_autotune_changes_timing_only():
     from pllcart3d_b200.solver import Solver
 
