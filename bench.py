@@ -335,7 +335,7 @@ def roofline_of(kernels, nprof, cells, precision, dims=None, form=None, explicit
 # committed under profiles/ (the bench itself runs only a few steps)
 GATE_RECORD = {
     "mixed": {"target": "c relative max-norm error <= 1e-5 after 1000 steps against the FP64 form",
-              "c_rel_after_1000_steps": 4.2e-3, "met": False,
+              "c_rel_after_1000_steps": 4.1e-3, "met": False,
               "record": "profiles/precision_forms_accuracy_fingering-512x256x256.md"},
     "mixed64": {"target": "c relative max-norm error <= 1e-5 after 1000 steps against the FP64 form",
                 "c_rel_after_1000_steps": 1.13e-6, "met": True,
