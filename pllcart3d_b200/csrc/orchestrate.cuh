@@ -92,7 +92,7 @@ void launch_explicit(pllgpu_ctx* ctx, const real* un, const real* vn, const real
     A.pg = VAR == VC ? nullptr : bufs<real>(ctx).pg[VAR];
     A.Hm = h_nm1<real>(ctx, VAR);
     A.H = h_n<real>(ctx, VAR);
-    A.S = (inc_t<real>*)bufs<real>(ctx).S;
+    A.S = bufs<real>(ctx).S;
     A.scal = ctx->scal;
     A.g = g;
     A.r = r;
@@ -201,8 +201,8 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
     X.qn = q_new<real>(ctx, VAR);
     X.H = h_n<real>(ctx, VAR);
     X.Hm = h_nm1<real>(ctx, VAR);
-    X.S = (inc_t<real>*)B.S;
-    X.cc = (inc_t<real>*)B.cc;
+    X.S = B.S;
+    X.cc = B.cc;
     X.scal = ctx->scal;
     X.g = g;
     X.r = r;
@@ -223,7 +223,7 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
         ydone = launch_line_seg<VAR, 1, real>(ctx, R, X);
         if (!ydone && VAR == VC && nj(R) <= ZP_MAX && nj(R) >= 2 * (ZP_MAX / 32) && !ctx->P.exact_dct) {
             go<k_adi_y_part_b<VAR, float>>(ctx, k_adi_y_part<VAR, float>, dim3((nk(R) + 31) / 32, ni(R)), 256,
-                                           adi_y_part_smem<float>(), ctx->G, R, ctx->K, X.mu, X.S, ctx->scal, alpha);
+                                           adi_y_part_smem<float>(), ctx->G, R, ctx->K, X.mu, B.S, ctx->scal, alpha);
             ydone = true;
         }
     }
@@ -236,14 +236,14 @@ void launch_implicit(pllgpu_ctx* ctx, double g, double r)
         if (nk(R) <= ZP_MAX && nk(R) >= 2 * (ZP_MAX / 32) && !ctx->P.exact_dct) {
             // the partitioned warp solve (precision form and FP64 form)
             go<k_adi_z_part_b<VAR, real>>(ctx, k_adi_z_part<VAR, real>, dim3((nj(R) + 3) / 4, ni(R)), 128, 0, ctx->G, R,
-                                          ctx->K, X.mu, X.S, ctx->scal, alpha);
+                                          ctx->K, X.mu, B.S, ctx->scal, alpha);
             zdone = true;
         }
     }
     if (!zdone) {
         constexpr size_t smem = adi_z_smem_bytes<VAR, real>();
         go<k_adi_z_tiled_b<VAR, real>>(ctx, k_adi_z_tiled<VAR, real>, dim3((nj(R) + 127) / 128, ni(R)), 128, smem,
-                                       ctx->G, R, ctx->K, X.mu, X.S, X.cc, ctx->scal, alpha);
+                                       ctx->G, R, ctx->K, X.mu, B.S, B.cc, ctx->scal, alpha);
     }
     mark(ctx, lz[VAR]);
     bool xdone = false;

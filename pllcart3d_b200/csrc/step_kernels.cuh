@@ -18,33 +18,12 @@
 #define PLL_FP64_EXACT 1
 #endif
 
-// 1 (the mixed64 form's translation unit): the increments -- the ADI
-// right-hand side S and the line solves' scratch -- are stored in FP32 while
-// the state and all arithmetic stay FP64.  Default: stored as the state.
-#ifndef PLL_INC_F32
-#define PLL_INC_F32 0
-#endif
-
 namespace pll {
 // internal linkage: each translation unit (and so each precision form with
 // its own contraction flags) owns its instantiations
 namespace {
 
 enum { MU_CELL_ = 0, MU_XY_ = 1, MU_XZ_ = 2, MU_YZ_ = 3 };
-
-// storage type of the increments of a form whose state is `real`
-template <typename real>
-struct IncOf {
-    using type = real;
-};
-#if PLL_INC_F32
-template <>
-struct IncOf<double> {
-    using type = float;
-};
-#endif
-template <typename real>
-using inc_t = typename IncOf<real>::type;
 
 // x / h as the reference divides; exact as x * (1/h) when h is a power of
 // two.  The precision form (FP32) always multiplies by the rounded 1/h.
@@ -406,7 +385,7 @@ struct ExplicitArgs {
     const real* pg;     // accumulated pressure gradient of the variable
     const real* Hm;     // explicit term of the previous substep
     real* H;            // explicit term of this substep (out)
-    inc_t<real>* S;     // right-hand side of the ADI solve (out)
+    real* S;            // right-hand side of the ADI solve (out)
     const double* scal; // device scalars (dt)
     double g, r, alpha; // RK3 gamma, rho and gamma+rho
 };
@@ -807,8 +786,8 @@ struct XsweepArgs {
     real* qn;            // q_new (out)
     real* H;             // explicit term (outflow plane written here)
     const real* Hm;      // previous explicit term
-    inc_t<real>* S;      // eliminated rhs from the y/z sweeps (scratch)
-    inc_t<real>* cc;     // scratch
+    real* S;             // eliminated rhs from the y/z sweeps (scratch)
+    real* cc;            // scratch
     const double* scal;  // dt, vbulk
     double g, r, alpha;
 };
@@ -837,7 +816,7 @@ constexpr size_t adi_z_smem_bytes()
 template <int VAR, typename real>
 __device__ __forceinline__ void k_adi_z_tiled_run(const uint3 blockIdx, const dim3 gridDim,
     Geo G, Rng R, Consts K, MuPtrs<real> mu,
-                                                     inc_t<real>* __restrict__ S, inc_t<real>* __restrict__ cc,
+                                                     real* __restrict__ S, real* __restrict__ cc,
                                                      const double* __restrict__ scal, double alpha)
 {
     constexpr int W = 32;
@@ -870,7 +849,7 @@ __device__ __forceinline__ void k_adi_z_tiled_run(const uint3 blockIdx, const di
     const int sy = (int)G.sy;
     auto fetch_fwd = [&](int k0) {
         const int nk = (n - k0) < ZW ? (n - k0) : ZW;
-        const inc_t<real>* Sb = S + base0 + k0;
+        const real* Sb = S + base0 + k0;
         const real* Mb = mz + base0 + k0 + moff;
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
@@ -884,8 +863,8 @@ __device__ __forceinline__ void k_adi_z_tiled_run(const uint3 blockIdx, const di
     };
     auto fetch_bwd = [&](int k0) {
         const int nk = (n - k0) < ZW ? (n - k0) : ZW;
-        const inc_t<real>* Sb = S + base0 + k0;
-        const inc_t<real>* Cb = cc + base0 + k0;
+        const real* Sb = S + base0 + k0;
+        const real* Cb = cc + base0 + k0;
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
             const int r = 2 * q + hr;
@@ -994,7 +973,7 @@ __device__ __forceinline__ void k_adi_z_tiled_run(const uint3 blockIdx, const di
 }
 template <int VAR, typename real>
 __global__ void __launch_bounds__(128, 4) k_adi_z_tiled(Geo G, Rng R, Consts K, MuPtrs<real> mu,
-                                                     inc_t<real>* __restrict__ S, inc_t<real>* __restrict__ cc,
+                                                     real* __restrict__ S, real* __restrict__ cc,
                                                      const double* __restrict__ scal, double alpha)
 {
     k_adi_z_tiled_run<VAR, real>(blockIdx, gridDim, G, R, K, mu, S, cc, scal, alpha);
@@ -1113,7 +1092,7 @@ __device__ __forceinline__ void zp_solve(const real* A, const real* B, const rea
 template <int VAR, typename real>
 __device__ __forceinline__ void k_adi_z_part_run(const uint3 blockIdx, const dim3 gridDim,
     Geo G, Rng R, Consts K, MuPtrs<real> mu,
-                                                    inc_t<real>* __restrict__ S, const double* __restrict__ scal,
+                                                    real* __restrict__ S, const double* __restrict__ scal,
                                                     double alpha)
 {
     constexpr int E = ZP_MAX / 32;   // rows per lane
@@ -1194,7 +1173,7 @@ __device__ __forceinline__ void k_adi_z_part_run(const uint3 blockIdx, const dim
 }
 template <int VAR, typename real>
 __global__ void __launch_bounds__(128) k_adi_z_part(Geo G, Rng R, Consts K, MuPtrs<real> mu,
-                                                    inc_t<real>* __restrict__ S, const double* __restrict__ scal,
+                                                    real* __restrict__ S, const double* __restrict__ scal,
                                                     double alpha)
 {
     k_adi_z_part_run<VAR, real>(blockIdx, gridDim, G, R, K, mu, S, scal, alpha);
@@ -1262,7 +1241,7 @@ constexpr size_t adi_y_part_smem() { return sizeof(real) * 2 * 32 * YP_PITCH; }
 template <int VAR, typename real>
 __device__ __forceinline__ void k_adi_y_part_run(const uint3 blockIdx, const dim3 gridDim,
     Geo G, Rng R, Consts K, MuPtrs<real> mu,
-                                                    inc_t<real>* __restrict__ S, const double* __restrict__ scal,
+                                                    real* __restrict__ S, const double* __restrict__ scal,
                                                     double alpha)
 {
     constexpr int E = ZP_MAX / 32;
@@ -1349,7 +1328,7 @@ __device__ __forceinline__ void k_adi_y_part_run(const uint3 blockIdx, const dim
 }
 template <int VAR, typename real>
 __global__ void __launch_bounds__(256) k_adi_y_part(Geo G, Rng R, Consts K, MuPtrs<real> mu,
-                                                    inc_t<real>* __restrict__ S, const double* __restrict__ scal,
+                                                    real* __restrict__ S, const double* __restrict__ scal,
                                                     double alpha)
 {
     k_adi_y_part_run<VAR, real>(blockIdx, gridDim, G, R, K, mu, S, scal, alpha);
@@ -1388,8 +1367,8 @@ __device__ __forceinline__ void k_line_pf_run(const uint3 blockIdx, const dim3 g
     constexpr int LO = Closure<VAR, AXIS>::lo, HI = Closure<VAR, AXIS>::hi;
     constexpr int OFF = LineCoef<VAR, AXIS>::off;
     const real* __restrict__ fam = VAR == VC ? nullptr : line_family<VAR, AXIS, real>(A.mu);
-    inc_t<real>* __restrict__ S = A.S;
-    inc_t<real>* __restrict__ cc = A.cc;
+    real* __restrict__ S = A.S;
+    real* __restrict__ cc = A.cc;
 
     real boun = 0;
     if (AXIS == 0) {
@@ -1631,7 +1610,7 @@ __device__ __forceinline__ void k_line_seg_run(const uint3 blockIdx, const dim3 
     const real dt = (real)A.scal[S_DT];
     const real fac = (real)(0.5 * A.scal[S_DT] * A.alpha);
     const real* __restrict__ fam = VAR == VC ? nullptr : line_family<VAR, AXIS, real>(A.mu);
-    inc_t<real>* __restrict__ S = A.S;
+    real* __restrict__ S = A.S;
     // this thread's row e of the tiles: mym[e * TS], myq[e * TS]
     real* mym = ls_dyn + threadIdx.x;
     real* myq = ls_dyn + (VAR != VC ? (RS + 1) * TS : 0) + threadIdx.x;
@@ -1654,7 +1633,7 @@ __device__ __forceinline__ void k_line_seg_run(const uint3 blockIdx, const dim3 
     }
     real rS[RS];
     {
-        const inc_t<real>* sp = S + seg;
+        const real* sp = S + seg;
 #pragma unroll
         for (int e = 0; e < RS; ++e) rS[e] = live ? sp[e * st] : (real)0;
     }
