@@ -256,14 +256,22 @@ __device__ real stale_d2(const real* __restrict__ q, const Geo& G, const Rng& R,
     return (real)0;
 }
 
-// c' = c / b', r' = r / b' of one Thomas step.  The precision form
-// multiplies by one approximate reciprocal (b' >= 1 for these diagonally
-// dominant systems, so __fdividef is accurate to 2 ulp).
+// c' = c / b', r' = r / b' of one Thomas step: the exact form divides
+// twice as the reference does; the FP64 forms divide once and multiply by
+// the reciprocal; the precision form multiplies by one approximate
+// reciprocal (b' >= 1 for these diagonally dominant systems, so __fdividef
+// is accurate to 2 ulp).
 template <typename real>
 __device__ __forceinline__ void thomas_div(real lc, real num, real bb, real& cm, real& rm)
 {
+#if !PLL_FP64_EXACT
+    const real ib = (real)1 / bb;
+    cm = lc * ib;
+    rm = num * ib;
+#else
     cm = lc / bb;
     rm = num / bb;
+#endif
 }
 
 template <>
