@@ -6,11 +6,14 @@
 
 One step = one full RK3-CN time step (pllcart3d.c:158-195) of the named
 seeded synthetic fingering workload (default fingering-512x256x256, the size
-the headline metric is quoted at).  Both precision forms are timed: the
-headline `value` is the precision form (FP32 state, split-TF32 DCT, FP64
-Poisson mode solve), the plain FP64 form is reported beside it
-(`fp64_form`, `mixed_over_fp64`).  Every state array is at least 141 MB,
-larger than the 126 MB L2, so no L2 flush is needed between steps.
+the headline metric is quoted at).  Three forms are timed (`--precision`):
+the headline `value` is the mixed64 form (FP64 state, FP32 WENO5 weights:
+the form within 1e-5 of the FP64 form in c after 1000 steps), the plain
+FP64 form and the FP32-state precision form are reported beside it
+(`fp64_form`, `mixed_form`, `mixed64_over_fp64`, `mixed_over_fp64`).  At
+512x256x256 a state array is 276 MB in FP64 (138 MB in FP32), above the
+126 MB L2, and a step moves tens of GB, so no L2 flush is needed between
+steps (`config.l2` states the figures of the run).
 
 --impl ours       the GPU step through the pllgpu_ C ABI (one CUDA graph per
                   step); `value` is device-timed with CUDA events on the
@@ -291,6 +294,16 @@ def tensor_peak():
 TRAFFIC_RATIO = {("k_explicit2", "fp32"): 1.05, ("k_explicit", "fp64"): 1.04, ("k_explicit_tma", "fp64"): 1.04}
 
 
+def l2_note(prm, form):
+    """How the timed steps stay clear of L2 reuse: the field size of the form
+    and the step's traffic against the 126 MB L2 (no flush between steps)."""
+    word = 4 if form == "mixed" else 8
+    field = float(prm.shape[0] * prm.shape[1] * prm.shape[2]) * word / 1e6
+    step = roofline.step_bytes(prm.cells, "fp32" if form == "mixed" else "fp64") / 1e6
+    return (f"no L2 flush: each field {field:.0f} MB, each step moves {step / 1e3:.1f} GB "
+            f"({step / 126:.0f}x the 126 MB L2)")
+
+
 def roofline_of(kernels, nprof, cells, precision, dims=None, form=None, explicit="auto"):
     """Roofline of the kernel family with the largest share of the step."""
     hbm, peak_kind = peaks()
@@ -449,7 +462,7 @@ def run_ours(args, ws, rank, local):
             "config": {"workload": wl.name, "grid": [prm.nx, prm.ny, prm.nz],
                        "precision": args.headline,
                        "parallelism": "replicas" if ws > 1 else "single",
-                       "l2": "inputs larger than L2 (each field >= 141 MB)"},
+                       "l2": l2_note(prm, args.headline)},
             "e2e": e2e, "gpu_launches": head["launches_per_step"] * args.steps,
             "roofline": head["roofline"], "step_roofline": head["step_roofline"],
             "cpu_baseline": cpu, "clocks": head["clocks"],
