@@ -26,11 +26,16 @@ namespace {
 enum { MU_CELL_ = 0, MU_XY_ = 1, MU_XZ_ = 2, MU_YZ_ = 3 };
 
 // x / h as the reference divides; exact as x * (1/h) when h is a power of
-// two.  The precision form (FP32) always multiplies by the rounded 1/h.
+// two.  The FP64 forms (within rounding of the reference, not its operation
+// order) and the precision form always multiply by the rounded 1/h.
 template <typename real>
 __device__ __forceinline__ real over_h(real x, double h, double ih, int pow2)
 {
+#if PLL_FP64_EXACT
     return pow2 ? x * (real)ih : x / (real)h;
+#else
+    return x * (real)ih;
+#endif
 }
 
 template <>
@@ -43,7 +48,11 @@ __device__ __forceinline__ float over_h<float>(float x, double, double ih, int)
 template <typename real>
 __device__ __forceinline__ real over_2h(real x, double h, double i2h, int pow2)
 {
+#if PLL_FP64_EXACT
     return pow2 ? x * (real)i2h : x / ((real)2.0 * (real)h);
+#else
+    return x * (real)i2h;
+#endif
 }
 
 template <>
