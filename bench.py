@@ -351,7 +351,7 @@ GATE_RECORD = {
               "c_rel_after_1000_steps": 4.1e-3, "met": False,
               "record": "profiles/precision_forms_accuracy_fingering-512x256x256.md"},
     "mixed64": {"target": "c relative max-norm error <= 1e-5 after 1000 steps against the FP64 form",
-                "c_rel_after_1000_steps": 1.13e-6, "met": True,
+                "c_rel_after_1000_steps": 2.0e-6, "met": True,
                 "record": "profiles/precision_forms_accuracy_fingering-512x256x256.md"},
 }
 
