@@ -178,7 +178,12 @@ __device__ __forceinline__ void k_cfl_run(const uint3 blockIdx, const dim3 gridD
         double uv = 0.5 * ((double)u[id] + (double)u[id + G.sx]);
         double vv = 0.5 * ((double)v[id] + (double)v[id + G.sy]);
         double wv = 0.5 * ((double)w[id] + (double)w[id + 1]);
+#if PLL_FP64_EXACT
         double cfl = (fabs(uv) / K.hx) + (fabs(vv) / K.hy) + (fabs(wv) / K.hz);
+#else
+        // the FP64 forms: reciprocal spacings, the fusions written out
+        double cfl = fma(fabs(wv), K.ihz, fma(fabs(vv), K.ihy, fabs(uv) * K.ihx));
+#endif
         if (!isfinite(cfl)) atomicOr(status, (int)ST_NAN);
         else m = cfl;
     }
@@ -645,15 +650,13 @@ __device__ __forceinline__ void k_poisson_x_run(const uint3 blockIdx, const dim3
                     if (gauge) lr -= c * 0.0;
                     else lb += c;
                 }
-                double cm, rm;
+                double cm, rm;   // the FP64 forms divide once (thomas_div)
                 if (m == 0) {
                     lb = lb - 0.0 * a;
-                    cm = c / lb;
-                    rm = (lr - 0.0 * a) / lb;
+                    thomas_div<double>(c, (lr - 0.0 * a), lb, cm, rm);
                 } else {
                     lb = (lb - cprev * a);
-                    cm = c / lb;
-                    rm = (lr - rprev * a) / lb;
+                    thomas_div<double>(c, (lr - rprev * a), lb, cm, rm);
                 }
                 cc[id] = cm;
                 rr[id] = rm;
