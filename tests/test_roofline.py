@@ -66,3 +66,16 @@ def test_bench_roofline_picks_the_largest_family():
     assert r64["kernel"] == "k_explicit_tma"
     assert abs(r64["traffic"] - bench.TRAFFIC_RATIO[("k_explicit_tma", "fp64")]
                * roofline.kernel_bytes_per_launch("explicit_u", cells, "fp64")) < 1.0
+
+
+def test_bench_states_its_l2_figures():
+    """The bench line's config.l2 note follows the run's own sizes: field
+    size in the form's word and the step's modelled traffic against L2."""
+    import bench
+    from pllcart3d_b200.params import workload
+
+    p = workload("fingering-512x256x256").params
+    assert bench.l2_note(p, "mixed64").startswith("no L2 flush: each field 276 MB, each step moves 81.3 GB")
+    assert "each field 138 MB" in bench.l2_note(p, "mixed")
+    small = workload("fingering-256x128x128").params
+    assert "each field 35 MB" in bench.l2_note(small, "fp64")
