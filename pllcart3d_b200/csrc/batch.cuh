@@ -156,15 +156,12 @@ struct LaunchRecT : LaunchRec {
     }
     cudaError_t prepare() const override
     {
+        // static and dynamic shared memory together above 48 KB need the
+        // opt-in, which is a per-device attribute: set on every build (a
+        // host call, once per recorded launch, never per step)
         const void* kb = batched_kernel();
-        // dynamic shared memory opted in so far (static and dynamic shared
-        // memory together above 48 KB need the opt-in)
-        static size_t opted = 0;
-        if (kb && smem > opted) {
-            if (cudaError_t e = cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))
-                return e;
-            opted = smem;
-        }
+        if (kb && smem > 0)
+            return cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         return cudaSuccess;
     }
     cudaError_t many(const unsigned char* tab, size_t stride, unsigned n, cudaStream_t st) const override
